@@ -1,0 +1,487 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 LPA-ICI denoiser; prints ONE JSON line (rank 0).
+
+Workload (one step): the plain single-image forward on a 4096x4096 FP32 synthetic image (polygons,
+linear ramp, 4-16 px stripes; RGBE-quantised; noise sigma = 20/255 from seed 20250910), 16 directions
+x 7 scales of the symmetric m=(1,0) kernel set, gamma = 2.  With --gpus N every rank denoises its own
+4096^2 image (weak scaling, no collective on the data path); `value` = all ranks' pixels / the slowest
+rank's time.
+
+  value     Mpix/s with the input resident in HBM, device time of the forward launch (CUDA events on
+            the launching stream), L2 flushed (256 MB write) between timed steps
+  e2e       the same metric through the C ABI's host-pointer entry (lpaici_denoise_host): pinned host
+            input -> H2D -> forward -> D2H -> host, synchronous, wall clock per step
+  roofline  FP32 issue bound: every tap is one multiply and one separately rounded add (bit-exact with
+            the reference), so the peak is the FP32 pipe's measured mul+add lane-op rate on this GPU
+            (probe in lib/liblpaici_bench.so); achieved = 2 x algorithmic taps / kernel time
+  cpu_baseline  the reference's own CPU engine (anisotropic_lpa_ici_cpu_fused of
+            src/v1_0_lpa_ici_2D_fused.cpp, compiled in-process into oracle/_ref/) on all host cores,
+            one 256x256 crop of the benchmark image per thread
+  extra     batched persistent forward over 64 images (sides U[256,2048], sigma U[10,40]/255, gamma
+            U[1.5,2.5]) in a CUDA graph, and the adjoint on 8 x 1024^2, each against the plain forward
+            on the same images
+
+--impl reference runs only the reference's CPU engine (bounded sample per step, all host threads).
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import gzip
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "lpa-ici-cuda_b200")
+sys.path.insert(0, PKG)
+
+METRIC = "Mpix/s at 4096^2 16x7: batched+adjoint vs plain on same GPU, max err<=1e-4"
+UNIT = "Mpix/s"
+SYM = "lpa_kernels_m_1_0_d_16_h12_1_2_4_8_16_24_32_symmetric.txt"
+SIGMA = float(np.float32(20.0) / np.float32(255.0))
+GAMMA = 2.0
+SEED = 20250910
+SIZE = 4096
+
+
+def kernel_path(name: str, tmp: str) -> str:
+    gz = os.path.join(ROOT, "tests", "golden", "kernels", name + ".gz")
+    out = os.path.join(tmp, name)
+    with gzip.open(gz, "rb") as f, open(out, "wb") as g:
+        shutil.copyfileobj(f, g)
+    return out
+
+
+def bench_image(size: int, seed: int, sigma: float):
+    import lpaici
+
+    clean = lpaici.synth_image(size, size, seed)
+    return clean, lpaici.add_noise(clean, sigma, SEED)
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                smax.append(float(f[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def fp32_peak() -> dict:
+    import ctypes as C
+
+    lib = C.CDLL(os.path.join(PKG, "lib", "liblpaici_bench.so"))
+    lib.lpaici_bench_fp32_peak.argtypes = [C.POINTER(C.c_double)]
+    r = (C.c_double * 3)()
+    if lib.lpaici_bench_fp32_peak(r) != 0:
+        raise RuntimeError("FP32 peak probe failed")
+    return {"ffma_lane_ops_per_s": r[0], "muladd_lane_ops_per_s": r[1], "muladd2_lane_ops_per_s": r[2]}
+
+
+def algorithmic_taps(torch, ks, smap) -> float:
+    """Taps the reference's fused loop convolves: for every (direction, pixel), all nonzero taps of
+    scales 0 .. min(s*+1, S-1) (the first rejected scale is convolved, then dropped)."""
+    nnz = torch.tensor(ks.nnz().reshape(ks.D, ks.S), dtype=torch.float64, device=smap.device)
+    prefix = torch.cumsum(nnz, dim=1)  # prefix[d, s] = taps of scales 0..s
+    stop = torch.clamp(smap.long() + 1, max=ks.S - 1)
+    total = 0.0
+    for d in range(ks.D):
+        total += float(prefix[d][stop[d]].sum())
+    return total
+
+
+def time_launches(torch, fn, steps: int, warmup: int, flush) -> list[float]:
+    """Per-step device milliseconds of fn() (events on the current stream), L2 flushed in between."""
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return ms
+
+
+def cpu_reference_sample(noisy: np.ndarray, crop: int, threads: int, sigma: float, gamma: float, seed: int = 0):
+    """The reference's CPU engine on `threads` distinct crop x crop pieces of `noisy`, one per thread,
+    each denoised as a whole image (as the reference's executables do).  Returns (Mpix/s, seconds)."""
+    import concurrent.futures as cf
+
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_bind as ob  # the reference compiled from its sources (oracle/_ref): timed, not shipped
+
+    H, W = noisy.shape
+    rng = np.random.default_rng(seed)
+    crops = []
+    for _ in range(threads):
+        y, x = (int(v) for v in rng.integers(0, [H - crop + 1, W - crop + 1]))
+        crops.append(np.ascontiguousarray(noisy[y:y + crop, x:x + crop]))
+    tmp = tempfile.mkdtemp()
+    with quiet_stdout():  # the reference prints progress lines on stdout: keep them off the JSON line
+        try:
+            k = ob.ref_load_kernels(kernel_path(SYM, tmp))
+        finally:
+            shutil.rmtree(tmp, ignore_errors=True)
+        var = ob.ref_variances(k, np.float32(sigma))
+        t0 = time.perf_counter()
+        with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+            list(ex.map(lambda c: ob.ref_forward(c, k, var, gamma), crops))
+        secs = time.perf_counter() - t0
+    return threads * crop * crop / secs / 1e6, secs
+
+
+class quiet_stdout:
+    """Sends file descriptor 1 to /dev/null (C and C++ writers included, buffers flushed both ways)."""
+
+    def __enter__(self):
+        import ctypes
+
+        self.libc = ctypes.CDLL(None)
+        sys.stdout.flush()
+        self.libc.fflush(None)
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+
+    def __exit__(self, *exc):
+        self.libc.fflush(None)
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+        return False
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_reference(args, rank: int, world: int) -> None:
+    if rank != 0:
+        return
+    threads = host_threads()
+    _, noisy = bench_image(SIZE, SEED, SIGMA)
+    for _ in range(args.warmup):
+        cpu_reference_sample(noisy, 64, threads, SIGMA, GAMMA, seed=1)
+    vals, secs = [], []
+    for i in range(args.steps):
+        v, s = cpu_reference_sample(noisy, args.ref_crop, threads, SIGMA, GAMMA, seed=100 + i)
+        vals.append(v)
+        secs.append(s)
+    value = float(np.mean(vals))
+    sample = (f"{threads} crops of {args.ref_crop}x{args.ref_crop} px of the 4096^2 benchmark image per step, "
+              f"one per host thread, each denoised as a whole image by anisotropic_lpa_ici_cpu_fused")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(secs)) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "plain LPA-ICI forward, 4096x4096 synthetic, sym 16x7, sigma 20/255, gamma 2",
+                   "reference": "titocapovilla/lpa-ici-cuda src/v1_0_lpa_ici_2D_fused.cpp (CPU, built -O3)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank: int, world: int, local_rank: int) -> None:
+    import torch
+
+    import lpaici
+
+    dist = world > 1
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    tmp = tempfile.mkdtemp()
+    ks = lpaici.KernelSet.load(kernel_path(SYM, tmp))
+    clean, noisy_h = bench_image(SIZE, SEED + rank, SIGMA)
+    x = torch.from_numpy(noisy_h).to(dev)
+    out = torch.empty_like(x)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
+
+    # untimed: tile autotune on this image, scale maps for the algorithmic tap count
+    best, tune_ms = ks.autotune(SIZE, SIZE, SIGMA, GAMMA, sample=x, reps=2)
+    _, smap = lpaici.forward(ks, x, SIGMA, GAMMA, out=out, scale_map=True)
+    torch.cuda.synchronize()
+    taps = algorithmic_taps(torch, ks, smap)
+    del smap
+
+    fwd = lambda: lpaici.forward(ks, x, SIGMA, GAMMA, out=out)  # noqa: E731
+    for _ in range(args.warmup):
+        fwd()
+    torch.cuda.synchronize()
+    if dist:
+        torch.distributed.barrier()
+    clocks = Clocks(local_rank)
+    clocks.start()
+    torch.cuda.synchronize()
+    if dist:
+        torch.distributed.barrier()
+    ms = time_launches(torch, fwd, args.steps, 0, flush)
+    torch.cuda.synchronize()
+    if dist:
+        torch.distributed.barrier()
+    clk = clocks.stop()
+    ms_step = float(np.mean(ms))
+    if dist:
+        t = torch.tensor([ms_step], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_step = float(t.item())
+    px = SIZE * SIZE
+    value = world * px / (ms_step * 1e-3) / 1e6
+
+    # parity of this run: two windows against the oracle (window + 31 px halo), bit for bit
+    parity = check_windows(torch, ks, noisy_h, out, rank) if rank == 0 and not args.no_parity else None
+
+    # e2e through the C ABI with pinned host buffers
+    pin_in = torch.from_numpy(noisy_h).pin_memory()
+    pin_out = torch.empty_like(pin_in).pin_memory()
+    host_in, host_out = pin_in.numpy(), pin_out.numpy()
+    for _ in range(max(1, args.warmup)):
+        lpaici.denoise_host(ks, host_in, SIGMA, GAMMA, out=host_out)
+    if dist:
+        torch.distributed.barrier()
+    e2e_s = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        lpaici.denoise_host(ks, host_in, SIGMA, GAMMA, out=host_out)
+        e2e_s.append(time.perf_counter() - t0)
+    e2e_step = float(np.mean(e2e_s))
+    if dist:
+        t = torch.tensor([e2e_step], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_step = float(t.item())
+    if not np.array_equal(host_out.view(np.uint32), out.cpu().numpy().view(np.uint32)):
+        raise RuntimeError("host-pointer path differs from the device path")
+
+    extra = None
+    peak = None
+    if rank == 0:
+        peak = fp32_peak()
+    if rank == 0 and world == 1 and not args.no_extras:
+        extra = run_extras(torch, lpaici, ks, args, flush)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = host_threads()
+        v, s = cpu_reference_sample(noisy_h, 256, threads, SIGMA, GAMMA)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
+               "sample": f"{threads} crops of 256x256 px of the benchmark image, one per host thread, each "
+                         f"denoised whole by the reference's anisotropic_lpa_ici_cpu_fused ({s:.1f} s)"}
+
+    if rank != 0:
+        if dist:
+            torch.distributed.barrier()
+        return
+    kernel_s = ms_step * 1e-3
+    peak_ops = max(peak["muladd_lane_ops_per_s"], peak["muladd2_lane_ops_per_s"])
+    achieved = 2.0 * taps / kernel_s  # one multiply + one add per tap
+    tw, th, thr, ppt = lpaici.tile_configs()[best]
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "plain LPA-ICI forward, one 4096x4096 synthetic image per GPU, sym 16x7 kernels, "
+                               "sigma 20/255, gamma 2",
+                   "image": "polygons + linear ramp + 4-16 px stripes, RGBE-quantised, seed 20250910 (+rank)",
+                   "l2": "flushed between timed steps (256 MB write)",
+                   "tile": {"config": best, "tile_w": tw, "tile_h": th, "threads": thr, "pixels_per_thread": ppt},
+                   "parallelism": f"dp{world} (independent images, no collective)"},
+        "roofline": {"bound": "fp32", "achieved": achieved / 1e12, "peak": peak_ops / 1e12, "unit": "TFLOP/s",
+                     "frac": achieved / peak_ops, "traffic": None,
+                     "note": "FLOP = 2 per algorithmic tap (mul + separately rounded add); peak = measured FP32 "
+                             "mul+add lane-op rate on this GPU",
+                     "algorithmic_taps_per_px": taps / px,
+                     "fp32_probe_tops": {k: v / 1e12 for k, v in peak.items()}},
+        "cpu_baseline": cpu,
+        "e2e": {"value": world * px / e2e_step / 1e6, "unit": UNIT, "h2d_bytes_per_step": px * 4,
+                "d2h_bytes_per_step": px * 4},
+        "gpu_launches": args.steps,
+        "clocks": clk,
+        "parity": parity,
+        "extra": extra,
+        "autotune_ms": [float(v) for v in tune_ms],
+    }
+    print(json.dumps(line), flush=True)
+    if dist:
+        torch.distributed.barrier()
+    shutil.rmtree(tmp, ignore_errors=True)
+
+
+def check_windows(torch, ks, noisy_h, out, rank):
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_bind as ob
+
+    tmp = tempfile.mkdtemp()
+    try:
+        ko = ob.oracle_load_kernels(kernel_path(SYM, tmp))
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    var = ks.variances(SIGMA)
+    got = out.cpu().numpy()
+    R, n, ok = ks.radius, 48, True
+    rng = np.random.default_rng(rank)
+    for y, x in [(0, 0)] + [tuple(int(v) for v in rng.integers(0, SIZE - n, 2))]:
+        y0, x0, y1, x1 = max(0, y - R), max(0, x - R), min(SIZE, y + n + R), min(SIZE, x + n + R)
+        ref, _, _ = ob.oracle_forward_f32(noisy_h[y0:y1, x0:x1], ko, var, GAMMA)
+        ok &= np.array_equal(got[y:y + n, x:x + n].view(np.uint32),
+                             ref[y - y0:y - y0 + n, x - x0:x - x0 + n].view(np.uint32))
+    return {"windows_vs_oracle": 2, "bit_exact": bool(ok)}
+
+
+def run_extras(torch, lpaici, ks, args, flush) -> dict:
+    import concurrent.futures as cf
+
+    rng = np.random.default_rng(SEED)
+    n = 64
+    dims = rng.integers(256, 2049, size=(n, 2))
+    sig = (rng.uniform(10, 40, n).astype(np.float32) / np.float32(255.0)).astype(np.float32)
+    gam = rng.uniform(1.5, 2.5, n).astype(np.float32)
+
+    def make(i):
+        w, h = int(dims[i, 0]), int(dims[i, 1])
+        return lpaici.add_noise(lpaici.synth_image(w, h, SEED + 1 + i), float(sig[i]), SEED + i)
+
+    with cf.ThreadPoolExecutor(max_workers=min(16, host_threads())) as ex:
+        hosts = list(ex.map(make, range(n)))
+    xs = [torch.from_numpy(h).cuda() for h in hosts]
+    outs = [torch.empty_like(x) for x in xs]
+    total_px = float(sum(h.size for h in hosts))
+    batch = lpaici.Batch(ks, xs, outs, [float(s) for s in sig], [float(g) for g in gam], use_graph=True)
+    steps = max(2, min(args.steps, 5))
+    b_ms = time_launches(torch, batch.run, steps, 1, flush)
+    singles = [torch.empty_like(x) for x in xs]
+
+    def plain():
+        for x, o, s, g in zip(xs, singles, sig, gam):
+            lpaici.forward(ks, x, float(s), float(g), out=o)
+
+    p_ms = time_launches(torch, plain, steps, 1, flush)
+    same = all(torch.equal(a.view(torch.int32), b.view(torch.int32)) for a, b in zip(outs, singles))
+    batch.close()
+    del xs, outs, singles
+
+    # adjoint: 8 x 1024^2, sigma 20/255, gamma 2, g ~ N(0, 1)
+    m = 8
+    xa = [torch.from_numpy(lpaici.add_noise(lpaici.synth_image(1024, 1024, SEED + 100 + i), SIGMA, SEED + i)).cuda()
+          for i in range(m)]
+    ga = [torch.randn(1024, 1024, generator=torch.Generator().manual_seed(i)).cuda() for i in range(m)]
+    gi = [torch.empty_like(x) for x in xa]
+    fo = [torch.empty_like(x) for x in xa]
+
+    def adj():
+        for x, g, o in zip(xa, ga, gi):
+            lpaici.backward(ks, x, g, SIGMA, GAMMA, grad_in=o)
+
+    def fwd8():
+        for x, o in zip(xa, fo):
+            lpaici.forward(ks, x, SIGMA, GAMMA, out=o)
+
+    a_ms = time_launches(torch, adj, steps, 1, flush)
+    f_ms = time_launches(torch, fwd8, steps, 1, flush)
+    return {
+        "batched": {"images": n, "mpix": total_px / 1e6, "value": total_px / (np.mean(b_ms) * 1e-3) / 1e6,
+                    "plain_same_images": total_px / (np.mean(p_ms) * 1e-3) / 1e6, "unit": UNIT,
+                    "graph": True, "bit_equal_to_plain": bool(same)},
+        "adjoint": {"images": m, "size": 1024, "value": m * 1024 * 1024 / (np.mean(a_ms) * 1e-3) / 1e6,
+                    "forward_same_images": m * 1024 * 1024 / (np.mean(f_ms) * 1e-3) / 1e6, "unit": UNIT,
+                    "adjoint_over_forward_time": float(np.mean(a_ms) / np.mean(f_ms))},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--ref-crop", type=int, default=256, help="crop side per thread for --impl reference")
+    ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import torch
+
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,344 @@
+// batched.cu -- many images of uneven sizes, sigmas and gammas in one persistent launch.
+//
+// The plan cuts every image into the tiles of one tile configuration and orders the tiles into a
+// single work queue, full tiles of the largest images first and partial edge tiles last, so the
+// cheap ragged tiles fill the tail.  A persistent grid (one wave: SMs x resident CTAs) stages the
+// kernel set in shared memory once per CTA, then pulls tile indices from a global atomic counter
+// until the queue is empty; there is no inter-CTA waiting of any kind.  With use_graph the counter
+// reset and the launch are captured once into a CUDA graph and replayed by lpaici_batch_run.
+// No reference counterpart: the reference denoises one image per process
+// (src/v4_1_lpa_ici_2D_sparse_shared.cu:365-530).
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "configs.h"
+#include "tile_core.cuh"
+
+namespace lpaici {
+
+// Per-image descriptor in device memory.
+struct BatchImage {
+    const float *in;
+    float *out;
+    uint8_t *smap;
+    int W, H, in_pitch, out_pitch;
+    int tab_offset;  // float index of var[nk] (thr[nk] follows) in the plan's table array
+    int pad;
+};
+
+struct BatchArgs {
+    const BatchImage *images;
+    const float *tables;    // per image var[nk], thr[nk]
+    const int2 *items;      // (image, tile index within the image)
+    int n_items;
+    unsigned *counter;      // work-queue head, zeroed before every launch
+    int D, S, R;
+    const int *blob;
+    int blob_words, run_word, weight_word;
+};
+
+template <int P, int WX, int WY>
+__global__ void __launch_bounds__(32 * WX * WY)
+    lpaici_batched_kernel(const __grid_constant__ BatchArgs a) {
+    using Shape = TileShape<P, WX, WY>;
+    extern __shared__ __align__(16) int smem[];
+    __shared__ int s_item;
+    const int nk = a.D * a.S;
+    const int tab_words = (2 * nk + 3) & ~3;
+    int *s_blob = smem;
+    float *s_var = reinterpret_cast<float *>(smem + a.blob_words);
+    float *s_thr = s_var + nk;
+    float *s_tile = reinterpret_cast<float *>(smem + a.blob_words + tab_words);
+    const TileGeom g = TileGeom::make(Shape::kTileW, Shape::kTileH, a.R);
+
+    stage_words(s_blob, a.blob, a.blob_words);
+    int cur_image = -1;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = static_cast<int>(atomicAdd(a.counter, 1u));
+        __syncthreads();  // s_item visible; previous tile's sweep finished before the tile is reloaded
+        const int item = s_item;
+        if (item >= a.n_items) break;
+        const int2 it = a.items[item];
+        const BatchImage bi = a.images[it.x];
+        if (it.x != cur_image) {
+            const float *t = a.tables + bi.tab_offset;
+            for (int i = threadIdx.x; i < nk; i += blockDim.x) {
+                s_var[i] = t[i];
+                s_thr[i] = t[nk + i];
+            }
+            cur_image = it.x;
+        }
+        const int tiles_x = (bi.W + Shape::kTileW - 1) / Shape::kTileW;
+        const int x0 = (it.y % tiles_x) * Shape::kTileW, y0 = (it.y / tiles_x) * Shape::kTileH;
+        ImageArgs img{};
+        img.in = bi.in;
+        img.out = bi.out;
+        img.gout = nullptr;
+        img.smap = bi.smap;
+        img.W = bi.W;
+        img.in_h = bi.H;
+        img.in_pitch = bi.in_pitch;
+        img.out_pitch = bi.out_pitch;
+        img.row_begin = 0;
+        img.rows_out = bi.H;
+        load_tile(s_tile, img, x0, y0, a.R, g);
+        __syncthreads();
+        sweep_tile<P, WX, WY>(img, x0, y0, a.D, a.S, a.R, g, s_blob, a.run_word, a.weight_word, s_var, s_thr, s_tile);
+        __syncthreads();  // everyone done with s_tile / s_item before the next tile
+    }
+}
+
+namespace {
+
+struct KernelInfo {
+    const void *fn;
+    int tile_w, tile_h, threads;
+    size_t smem;
+};
+
+template <int P, int WX, int WY>
+int batched_info(const KernelTables &tab, KernelInfo *info) {
+    using Shape = TileShape<P, WX, WY>;
+    const TileGeom g = TileGeom::make(Shape::kTileW, Shape::kTileH, tab.R);
+    const int nk = tab.D * tab.S;
+    info->fn = reinterpret_cast<const void *>(lpaici_batched_kernel<P, WX, WY>);
+    info->tile_w = Shape::kTileW;
+    info->tile_h = Shape::kTileH;
+    info->threads = Shape::kThreads;
+    info->smem = sizeof(int) * (tab.blob_words + ((2 * nk + 3) & ~3)) + sizeof(float) * g.pitch * g.rows;
+    return LPAICI_OK;
+}
+
+int get_info(int config, const KernelTables &tab, KernelInfo *info) {
+#define LPAICI_BATCH_CASE(idx, P, WX, WY) \
+    case idx: return batched_info<P, WX, WY>(tab, info);
+    switch (config) {
+        LPAICI_TILE_CONFIGS(LPAICI_BATCH_CASE)
+        default: return set_error(LPAICI_ERR_INVALID_ARG, "tile config %d out of range", config);
+    }
+#undef LPAICI_BATCH_CASE
+}
+
+}  // namespace
+}  // namespace lpaici
+
+using namespace lpaici;
+
+struct lpaici_batch {
+    int device = -1;
+    KernelInfo info{};
+    BatchArgs args{};
+    int grid = 0;
+    void *dev_mem = nullptr;  // images | tables | items | counter
+    bool use_graph = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+int enqueue(lpaici_batch *b, cudaStream_t stream) {
+    cudaError_t e = cudaMemsetAsync(b->args.counter, 0, sizeof(unsigned), stream);
+    if (e != cudaSuccess) return cuda_error(e, "cudaMemsetAsync(queue counter)");
+    void *params[] = {&b->args};
+    e = cudaLaunchKernel(b->info.fn, dim3(b->grid), dim3(b->info.threads), params, b->info.smem, stream);
+    if (e != cudaSuccess) return cuda_error(e, "batched launch");
+    return LPAICI_OK;
+}
+
+void free_batch(lpaici_batch *b) {
+    if (!b) return;
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    if (b->dev_mem) cudaFree(b->dev_mem);
+    delete b;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lpaici_batch_create(const lpaici_kernelset *ks, const lpaici_image *images, int n, const lpaici_batch_options *opts,
+                        lpaici_stream_t stream_, lpaici_batch **out) {
+    if (!ks || !images || n <= 0 || !out) return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_batch_create: bad argument");
+    *out = nullptr;
+    cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+    const int nk = ks->D * ks->S;
+    for (int i = 0; i < n; i++) {
+        const lpaici_image &im = images[i];
+        if (!im.noisy || !im.denoised || im.width <= 0 || im.height <= 0 || im.noisy_pitch < im.width ||
+            im.out_pitch < im.width)
+            return set_error(LPAICI_ERR_INVALID_ARG, "batch image %d: bad pointer or size", i);
+        if (!(im.sigma > 0.0f) || !(im.gamma > 0.0f))
+            return set_error(LPAICI_ERR_INVALID_ARG, "batch image %d: sigma and gamma need positive numbers", i);
+    }
+    const int *blob = nullptr;
+    int rc = device_blob(ks, &blob);
+    if (rc != LPAICI_OK) return rc;
+    const int config = (opts && opts->tile_config >= 0) ? opts->tile_config : default_config(ks);
+
+    auto *b = new lpaici_batch();
+    cudaGetDevice(&b->device);
+    KernelTables tab;
+    fill_tables(ks, nullptr, 1.0f, 1.0f, &tab);
+    tab.blob = blob;
+    rc = get_info(config, tab, &b->info);
+    if (rc != LPAICI_OK) {
+        free_batch(b);
+        return rc;
+    }
+
+    // host images: descriptors, tables, and the ordered work queue
+    std::vector<BatchImage> imgs(n);
+    std::vector<float> tables(static_cast<size_t>(n) * 2 * nk);
+    struct Item {
+        int image, tile;
+        long key;
+    };
+    std::vector<Item> items;
+    for (int i = 0; i < n; i++) {
+        const lpaici_image &im = images[i];
+        KernelTables t;
+        fill_tables(ks, nullptr, im.sigma, im.gamma, &t);
+        std::memcpy(&tables[static_cast<size_t>(i) * 2 * nk], t.var, sizeof(float) * nk);
+        std::memcpy(&tables[static_cast<size_t>(i) * 2 * nk + nk], t.thr, sizeof(float) * nk);
+        imgs[i] = BatchImage{im.noisy, im.denoised, im.scale_map, im.width, im.height, im.noisy_pitch, im.out_pitch,
+                             i * 2 * nk, 0};
+        const int tx = (im.width + b->info.tile_w - 1) / b->info.tile_w;
+        const int ty = (im.height + b->info.tile_h - 1) / b->info.tile_h;
+        const long area = static_cast<long>(im.width) * im.height;
+        for (int y = 0; y < ty; y++)
+            for (int x = 0; x < tx; x++) {
+                const int w = std::min(b->info.tile_w, im.width - x * b->info.tile_w);
+                const int h = std::min(b->info.tile_h, im.height - y * b->info.tile_h);
+                // full tiles first, then by image size (largest first), then raster order
+                items.push_back({i, y * tx + x, static_cast<long>(w) * h * (1L << 40) + area});
+            }
+    }
+    std::stable_sort(items.begin(), items.end(), [](const Item &p, const Item &q) { return p.key > q.key; });
+    std::vector<int2> qitems(items.size());
+    for (size_t j = 0; j < items.size(); j++) qitems[j] = make_int2(items[j].image, items[j].tile);
+
+    const size_t img_bytes = sizeof(BatchImage) * n;
+    const size_t tab_off = (img_bytes + 255) & ~size_t(255);
+    const size_t tab_bytes = sizeof(float) * tables.size();
+    const size_t item_off = (tab_off + tab_bytes + 255) & ~size_t(255);
+    const size_t item_bytes = sizeof(int2) * qitems.size();
+    const size_t ctr_off = (item_off + item_bytes + 255) & ~size_t(255);
+    const size_t total = ctr_off + 256;
+    cudaError_t e = cudaMalloc(&b->dev_mem, total);
+    if (e != cudaSuccess) {
+        free_batch(b);
+        return cuda_error(e, "cudaMalloc(batch plan)");
+    }
+    char *base = static_cast<char *>(b->dev_mem);
+    e = cudaMemcpy(base, imgs.data(), img_bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(base + tab_off, tables.data(), tab_bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(base + item_off, qitems.data(), item_bytes, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        free_batch(b);
+        return cuda_error(e, "cudaMemcpy(batch plan)");
+    }
+    b->args.images = reinterpret_cast<const BatchImage *>(base);
+    b->args.tables = reinterpret_cast<const float *>(base + tab_off);
+    b->args.items = reinterpret_cast<const int2 *>(base + item_off);
+    b->args.n_items = static_cast<int>(qitems.size());
+    b->args.counter = reinterpret_cast<unsigned *>(base + ctr_off);
+    b->args.D = ks->D;
+    b->args.S = ks->S;
+    b->args.R = ks->radius;
+    b->args.blob = blob;
+    b->args.blob_words = tab.blob_words;
+    b->args.run_word = tab.run_word;
+    b->args.weight_word = tab.weight_word;
+
+    int max_optin = 0, sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+    if (b->info.smem > static_cast<size_t>(max_optin)) {
+        free_batch(b);
+        return set_error(LPAICI_ERR_UNSUPPORTED, "batched tile needs %zu B of shared memory, device allows %d",
+                         b->info.smem, max_optin);
+    }
+    e = cudaFuncSetAttribute(b->info.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(b->info.smem));
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, b->info.fn, b->info.threads, b->info.smem);
+    if (e != cudaSuccess || per_sm <= 0) {
+        free_batch(b);
+        return e != cudaSuccess ? cuda_error(e, "batched occupancy")
+                                : set_error(LPAICI_ERR_UNSUPPORTED, "batched kernel does not fit on an SM");
+    }
+    b->grid = std::min(sms * per_sm, b->args.n_items);
+
+    b->use_graph = opts && opts->use_graph;
+    if (b->use_graph) {
+        cudaStream_t cap = nullptr;
+        e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            rc = enqueue(b, cap);
+            cudaError_t e2 = cudaStreamEndCapture(cap, &b->graph);
+            if (rc == LPAICI_OK && e2 != cudaSuccess) rc = cuda_error(e2, "cudaStreamEndCapture");
+            if (rc == LPAICI_OK) {
+                e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+                if (e != cudaSuccess) rc = cuda_error(e, "cudaGraphInstantiate");
+            }
+        } else {
+            rc = cuda_error(e, "graph capture");
+        }
+        if (cap) cudaStreamDestroy(cap);
+        if (rc != LPAICI_OK) {
+            free_batch(b);
+            return rc;
+        }
+        e = cudaGraphUpload(b->exec, stream);
+        if (e != cudaSuccess) {
+            free_batch(b);
+            return cuda_error(e, "cudaGraphUpload");
+        }
+    }
+    *out = b;
+    return LPAICI_OK;
+}
+
+int lpaici_batch_run(lpaici_batch *b, lpaici_stream_t stream_) {
+    if (!b) return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_batch_run: null plan");
+    cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+    int dev = -1;
+    cudaGetDevice(&dev);
+    if (dev != b->device)
+        return set_error(LPAICI_ERR_INVALID_ARG, "batch planned on device %d, current device is %d", b->device, dev);
+    if (b->use_graph) {
+        cudaError_t e = cudaGraphLaunch(b->exec, stream);
+        if (e != cudaSuccess) return cuda_error(e, "cudaGraphLaunch");
+        return LPAICI_OK;
+    }
+    return enqueue(b, stream);
+}
+
+int lpaici_batch_destroy(lpaici_batch *b) {
+    if (b) {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        cudaSetDevice(b->device);
+        cudaDeviceSynchronize();
+        free_batch(b);
+        if (cur >= 0) cudaSetDevice(cur);
+    }
+    return LPAICI_OK;
+}
+
+int lpaici_forward_batched(const lpaici_kernelset *ks, const lpaici_image *images, int n, lpaici_stream_t stream) {
+    lpaici_batch *b = nullptr;
+    lpaici_batch_options opts{0, -1};
+    int rc = lpaici_batch_create(ks, images, n, &opts, stream, &b);
+    if (rc != LPAICI_OK) return rc;
+    rc = lpaici_batch_run(b, stream);
+    cudaError_t e = cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream));
+    if (rc == LPAICI_OK && e != cudaSuccess) rc = cuda_error(e, "cudaStreamSynchronize");
+    free_batch(b);
+    return rc;
+}
+
+}  // extern "C"

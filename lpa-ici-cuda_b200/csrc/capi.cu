@@ -1,0 +1,333 @@
+// capi.cu -- C ABI entry points for the forward path, the reference-shaped host engine and the
+// tile-configuration table.
+#include <chrono>
+#include <cmath>
+#include <cstring>
+
+#include "configs.h"
+#include "internal.h"
+
+using namespace lpaici;
+
+namespace lpaici {
+
+int default_config(const lpaici_kernelset *ks) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) {
+        std::lock_guard<std::mutex> lock(ks->mu);
+        if (dev < static_cast<int>(ks->tuned_config.size()) && ks->tuned_config[dev] >= 0)
+            return ks->tuned_config[dev];
+    }
+    return LPAICI_DEFAULT_TILE_CONFIG;
+}
+
+static int check_params(float sigma_or_one, float gamma) {
+    if (!(sigma_or_one > 0.0f) || !std::isfinite(sigma_or_one))
+        return set_error(LPAICI_ERR_INVALID_ARG, "sigma needs a positive number, got %g", sigma_or_one);
+    if (!(gamma > 0.0f) || !std::isfinite(gamma))
+        return set_error(LPAICI_ERR_INVALID_ARG, "gamma needs a positive number, got %g", gamma);
+    return LPAICI_OK;
+}
+
+// Shared body of the forward entry points.
+static int forward_common(const lpaici_kernelset *ks, const float *d_in, int in_pitch, int width, int in_height,
+                          int row_begin, int row_count, float *d_out, int out_pitch, const float *host_var,
+                          float sigma, float gamma, uint8_t *d_smap, cudaStream_t stream) {
+    if (!ks || !d_in || !d_out) return set_error(LPAICI_ERR_INVALID_ARG, "forward: null kernel set or image pointer");
+    if (width <= 0 || in_height <= 0 || row_count <= 0)
+        return set_error(LPAICI_ERR_INVALID_ARG, "forward: non-positive size %d x %d", width, row_count);
+    if (in_pitch < width || out_pitch < width)
+        return set_error(LPAICI_ERR_INVALID_ARG, "forward: pitch smaller than width");
+    if (row_begin < 0 || row_begin + row_count > in_height)
+        return set_error(LPAICI_ERR_INVALID_ARG, "forward: output rows [%d, %d) outside the %d input rows", row_begin,
+                         row_begin + row_count, in_height);
+    int rc = check_params(host_var ? 1.0f : sigma, gamma);
+    if (rc != LPAICI_OK) return rc;
+    if (host_var)
+        for (int k = 0; k < ks->D * ks->S; k++)
+            if (!(host_var[k] >= 0.0f))
+                return set_error(LPAICI_ERR_INVALID_ARG, "forward: variance %d is %g", k, host_var[k]);
+    const int *blob = nullptr;
+    rc = device_blob(ks, &blob);
+    if (rc != LPAICI_OK) return rc;
+    ImageArgs img{};
+    img.in = d_in;
+    img.out = d_out;
+    img.gout = nullptr;
+    img.smap = d_smap;
+    img.W = width;
+    img.in_h = in_height;
+    img.in_pitch = in_pitch;
+    img.out_pitch = out_pitch;
+    img.gout_pitch = 0;
+    img.row_begin = row_begin;
+    img.rows_out = row_count;
+    KernelTables tab;
+    fill_tables(ks, host_var, sigma, gamma, &tab);
+    tab.blob = blob;
+    return launch_forward(ks, img, tab, default_config(ks), stream);
+}
+
+}  // namespace lpaici
+
+extern "C" {
+
+int lpaici_forward(const lpaici_kernelset *ks, const float *d_noisy, int noisy_pitch, float *d_denoised,
+                   int out_pitch, int width, int height, float sigma, float gamma, uint8_t *d_scale_map,
+                   lpaici_stream_t stream) {
+    return forward_common(ks, d_noisy, noisy_pitch, width, height, 0, height, d_denoised, out_pitch, nullptr, sigma,
+                          gamma, d_scale_map, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int lpaici_forward_var(const lpaici_kernelset *ks, const float *d_noisy, int noisy_pitch, float *d_denoised,
+                       int out_pitch, int width, int height, const float *host_var, float gamma,
+                       uint8_t *d_scale_map, lpaici_stream_t stream) {
+    if (!host_var) return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_forward_var: null variances");
+    return forward_common(ks, d_noisy, noisy_pitch, width, height, 0, height, d_denoised, out_pitch, host_var, 1.0f,
+                          gamma, d_scale_map, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int lpaici_forward_rows(const lpaici_kernelset *ks, const float *d_in, int in_pitch, int width, int in_height,
+                        int row_begin, int row_count, float *d_out, int out_pitch, float sigma, float gamma,
+                        uint8_t *d_scale_map, lpaici_stream_t stream) {
+    return forward_common(ks, d_in, in_pitch, width, in_height, row_begin, row_count, d_out, out_pitch, nullptr, sigma,
+                          gamma, d_scale_map, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int lpaici_num_tile_configs(void) { return LPAICI_NUM_TILE_CONFIGS; }
+
+int lpaici_tile_config_desc(int index, int *tile_w, int *tile_h, int *threads, int *pixels_per_thread) {
+#define LPAICI_DESC_CASE(idx, P, WX, WY)                  \
+    case idx:                                             \
+        if (tile_w) *tile_w = (WX) * 4 * (P);             \
+        if (tile_h) *tile_h = (WY) * 8;                   \
+        if (threads) *threads = 32 * (WX) * (WY);         \
+        if (pixels_per_thread) *pixels_per_thread = (P);  \
+        return LPAICI_OK;
+    switch (index) {
+        LPAICI_TILE_CONFIGS(LPAICI_DESC_CASE)
+        default: return set_error(LPAICI_ERR_INVALID_ARG, "tile config %d out of range", index);
+    }
+#undef LPAICI_DESC_CASE
+}
+
+// ---- host-pointer engines ---------------------------------------------------------------------
+
+namespace {
+// Device buffers of lpaici_denoise_host, per thread and device.
+struct HostBuffers {
+    int dev = -1;
+    float *in = nullptr, *out = nullptr;
+    size_t cap = 0;
+    ~HostBuffers() { release(); }
+    void release() {
+        if (dev >= 0) {
+            int cur = -1;
+            cudaGetDevice(&cur);
+            cudaSetDevice(dev);
+            cudaFree(in);
+            cudaFree(out);
+            if (cur >= 0) cudaSetDevice(cur);
+        }
+        in = out = nullptr;
+        cap = 0;
+        dev = -1;
+    }
+};
+thread_local HostBuffers t_bufs;
+}  // namespace
+
+int lpaici_denoise_host(const lpaici_kernelset *ks, const float *host_noisy, float *host_denoised, int width,
+                        int height, float sigma, float gamma, lpaici_stream_t stream_) {
+    if (!ks || !host_noisy || !host_denoised || width <= 0 || height <= 0)
+        return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_denoise_host: bad argument");
+    cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_error(e, "cudaGetDevice");
+    const size_t n = static_cast<size_t>(width) * height;
+    if (t_bufs.dev != dev || t_bufs.cap < n) {
+        t_bufs.release();
+        e = cudaMalloc(&t_bufs.in, n * sizeof(float));
+        if (e == cudaSuccess) e = cudaMalloc(&t_bufs.out, n * sizeof(float));
+        if (e != cudaSuccess) {
+            t_bufs.release();
+            return cuda_error(e, "cudaMalloc(host buffers)");
+        }
+        t_bufs.dev = dev;
+        t_bufs.cap = n;
+    }
+    e = cudaMemcpyAsync(t_bufs.in, host_noisy, n * sizeof(float), cudaMemcpyHostToDevice, stream);
+    if (e != cudaSuccess) return cuda_error(e, "cudaMemcpyAsync(H2D)");
+    int rc = forward_common(ks, t_bufs.in, width, width, height, 0, height, t_bufs.out, width, nullptr, sigma, gamma,
+                            nullptr, stream);
+    if (rc != LPAICI_OK) return rc;
+    e = cudaMemcpyAsync(host_denoised, t_bufs.out, n * sizeof(float), cudaMemcpyDeviceToHost, stream);
+    if (e != cudaSuccess) return cuda_error(e, "cudaMemcpyAsync(D2H)");
+    e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return cuda_error(e, "cudaStreamSynchronize");
+    return LPAICI_OK;
+}
+
+int lpaici_release_host_buffers(void) {
+    t_bufs.release();
+    return LPAICI_OK;
+}
+
+int lpaici_anisotropic_gpu_fused(float *host_img_noisy, float *host_img_denoised, int width, int height, int channels,
+                                 float *host_global_weights_buffer, int num_dirs, int num_scales,
+                                 float *host_kernel_weights, int host_kernel_weights_size, int *host_offsets,
+                                 int *host_rows, int *host_cols, float *host_kernel_variances, float ici_gamma,
+                                 double *seconds) {
+    (void)host_global_weights_buffer;
+    if (channels != 1) return set_error(LPAICI_ERR_INVALID_ARG, "channels must be 1, got %d", channels);
+    if (!host_img_noisy || !host_img_denoised || !host_kernel_weights || !host_offsets || !host_rows || !host_cols ||
+        !host_kernel_variances || width <= 0 || height <= 0)
+        return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_anisotropic_gpu_fused: bad argument");
+    const long nk = static_cast<long>(num_dirs) * num_scales;
+    for (long k = 0; k < nk; k++)
+        if (host_offsets[k] < 0 || static_cast<long>(host_offsets[k]) + static_cast<long>(host_rows[k]) * host_cols[k] >
+                                       host_kernel_weights_size)
+            return set_error(LPAICI_ERR_KERNEL_FORMAT, "kernel %ld lies outside the %d weights", k,
+                             host_kernel_weights_size);
+    lpaici_kernelset *ks = nullptr;
+    int rc = lpaici_kernelset_create(host_kernel_weights, host_offsets, host_rows, host_cols, num_dirs, num_scales, &ks);
+    if (rc != LPAICI_OK) return rc;
+    const size_t n = static_cast<size_t>(width) * height;
+    float *d_in = nullptr, *d_out = nullptr;
+    cudaError_t e = cudaMalloc(&d_in, n * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&d_out, n * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemcpy(d_in, host_img_noisy, n * sizeof(float), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        rc = cuda_error(e, "lpaici_anisotropic_gpu_fused setup");
+    } else {
+        cudaDeviceSynchronize();
+        const auto t0 = std::chrono::steady_clock::now();  // the reference's window starts here (:1216)
+        rc = forward_common(ks, d_in, width, width, height, 0, height, d_out, width, host_kernel_variances, 1.0f,
+                            ici_gamma, nullptr, nullptr);
+        if (rc == LPAICI_OK) {
+            e = cudaMemcpy(host_img_denoised, d_out, n * sizeof(float), cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess) rc = cuda_error(e, "cudaMemcpy(D2H)");
+        }
+        const auto t1 = std::chrono::steady_clock::now();  // ... and ends after the copy back (:1240)
+        if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+    }
+    cudaFree(d_in);
+    cudaFree(d_out);
+    lpaici_kernelset_destroy(ks);
+    return rc;
+}
+
+}  // extern "C"
+
+// ---- autotuner ----------------------------------------------------------------------------------
+
+namespace {
+
+// Built-in tuning image: a smooth ramp, a stripe texture and blocks, plus hash noise of 0.08.
+__global__ void synth_tuning_image(float *img, int W, int H, int pitch) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= W || y >= H) return;
+    unsigned h = static_cast<unsigned>(x) * 0x9E3779B1u ^ static_cast<unsigned>(y) * 0x85EBCA77u;
+    h ^= h >> 15;
+    h *= 0x2C1B3C6Du;
+    h ^= h >> 12;
+    const float u = (h & 0xFFFFFF) * (1.0f / 16777216.0f) - 0.5f;
+    const float ramp = 0.3f * x / W + 0.2f * y / H;
+    const float stripes = 0.2f * sinf(0.7f * x + 0.4f * y);
+    const float block = (((x >> 7) ^ (y >> 7)) & 1) ? 0.3f : 0.0f;
+    img[static_cast<size_t>(y) * pitch + x] = ramp + stripes + block + 0.28f * u;
+}
+
+}  // namespace
+
+extern "C" int lpaici_autotune(lpaici_kernelset *ks, const float *d_sample, int width, int height, int pitch,
+                               float sigma, float gamma, int reps, int *best_config, float *ms_out,
+                               lpaici_stream_t stream_) {
+    if (!ks || width <= 0 || height <= 0 || (d_sample && pitch < width) || reps <= 0)
+        return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_autotune: bad argument");
+    int rc = check_params(sigma, gamma);
+    if (rc != LPAICI_OK) return rc;
+    cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+    const size_t n = static_cast<size_t>(width) * height;
+    float *in = nullptr, *out = nullptr;
+    cudaError_t e = cudaSuccess;
+    if (!d_sample) {
+        e = cudaMalloc(&in, n * sizeof(float));
+        if (e != cudaSuccess) return cuda_error(e, "cudaMalloc(autotune)");
+        synth_tuning_image<<<dim3((width + 255) / 256, height), 256, 0, stream>>>(in, width, height, width);
+        pitch = width;
+    }
+    e = cudaMalloc(&out, n * sizeof(float));
+    if (e != cudaSuccess) {
+        cudaFree(in);
+        return cuda_error(e, "cudaMalloc(autotune)");
+    }
+    const float *src = d_sample ? d_sample : in;
+    const int *blob = nullptr;
+    rc = device_blob(ks, &blob);
+    ImageArgs img{};
+    img.in = src;
+    img.out = out;
+    img.W = width;
+    img.in_h = height;
+    img.in_pitch = pitch;
+    img.out_pitch = width;
+    img.rows_out = height;
+    KernelTables tab;
+    fill_tables(ks, nullptr, sigma, gamma, &tab);
+    tab.blob = blob;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best_ms = 0.0f;
+    int best = -1;
+    for (int c = 0; rc == LPAICI_OK && c < LPAICI_NUM_TILE_CONFIGS; c++) {
+        int crc = launch_forward(ks, img, tab, c, stream);  // warm-up
+        if (crc != LPAICI_OK) {
+            if (ms_out) ms_out[c] = -1.0f;
+            if (crc == LPAICI_ERR_UNSUPPORTED) continue;  // this tile does not fit for this kernel set
+            rc = crc;
+            break;
+        }
+        cudaEventRecord(e0, stream);
+        for (int r = 0; r < reps && crc == LPAICI_OK; r++) crc = launch_forward(ks, img, tab, c, stream);
+        cudaEventRecord(e1, stream);
+        e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) {
+            rc = cuda_error(e, "autotune");
+            break;
+        }
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms /= reps;
+        if (ms_out) ms_out[c] = ms;
+        if (best < 0 || ms < best_ms) {
+            best = c;
+            best_ms = ms;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(in);
+    cudaFree(out);
+    if (rc != LPAICI_OK) return rc;
+    if (best < 0) return set_error(LPAICI_ERR_UNSUPPORTED, "no tile configuration fits this kernel set");
+    if (best_config) *best_config = best;
+    return lpaici_set_tile_config(ks, best);
+}
+
+extern "C" int lpaici_set_tile_config(lpaici_kernelset *ks, int config) {
+    if (!ks || config < -1 || config >= LPAICI_NUM_TILE_CONFIGS)
+        return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_set_tile_config: bad argument");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_error(e, "cudaGetDevice");
+    std::lock_guard<std::mutex> lock(ks->mu);
+    if (static_cast<int>(ks->tuned_config.size()) <= dev) {
+        ks->dev_blob.resize(dev + 1, nullptr);
+        ks->tuned_config.resize(dev + 1, -1);
+    }
+    ks->tuned_config[dev] = config;
+    return LPAICI_OK;
+}

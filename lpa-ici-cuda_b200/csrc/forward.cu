@@ -1,0 +1,78 @@
+// forward.cu -- single-image LPA-ICI forward: one launch, one CTA per output tile, all directions
+// and scales of the tile inside the CTA, aggregation in registers.
+//
+// Replaces the directional loop of anisotropic_lpa_ici_gpu_fused
+// (src/v4_1_lpa_ici_2D_sparse_shared.cu:1216-1235), i.e. 16 launches of
+// process_direction_fused_kernel (:1007-1092) + accumulate_direction_kernel (:1104-1111) and one
+// normalize_estimate_kernel (:1113-1120), with the kernel set read from global memory (staged in
+// shared memory per CTA) instead of capacity-limited constant memory.
+#include "tile_core.cuh"
+#include "configs.h"
+
+namespace lpaici {
+
+template <int P, int WX, int WY>
+__global__ void __launch_bounds__(32 * WX * WY)
+    lpaici_forward_kernel(const __grid_constant__ ImageArgs img, const __grid_constant__ KernelTables tab) {
+    using Shape = TileShape<P, WX, WY>;
+    extern __shared__ __align__(16) int smem[];
+    const int nk = tab.D * tab.S;
+    const int tab_words = (2 * nk + 3) & ~3;
+    int *s_blob = smem;
+    float *s_var = reinterpret_cast<float *>(smem + tab.blob_words);
+    float *s_thr = s_var + nk;
+    float *s_tile = reinterpret_cast<float *>(smem + tab.blob_words + tab_words);
+    const TileGeom g = TileGeom::make(Shape::kTileW, Shape::kTileH, tab.R);
+    const int x0 = blockIdx.x * Shape::kTileW, y0 = blockIdx.y * Shape::kTileH;
+
+    stage_words(s_blob, tab.blob, tab.blob_words);
+    for (int i = threadIdx.x; i < nk; i += blockDim.x) {
+        s_var[i] = tab.var[i];
+        s_thr[i] = tab.thr[i];
+    }
+    load_tile(s_tile, img, x0, y0, tab.R, g);
+    __syncthreads();
+    sweep_tile<P, WX, WY>(img, x0, y0, tab.D, tab.S, tab.R, g, s_blob, tab.run_word, tab.weight_word, s_var, s_thr,
+                          s_tile);
+}
+
+namespace {
+
+template <int P, int WX, int WY>
+int launch_cfg(const ImageArgs &img, const KernelTables &tab, cudaStream_t stream) {
+    using Shape = TileShape<P, WX, WY>;
+    const TileGeom g = TileGeom::make(Shape::kTileW, Shape::kTileH, tab.R);
+    const int nk = tab.D * tab.S;
+    const size_t smem = sizeof(int) * (tab.blob_words + ((2 * nk + 3) & ~3)) + sizeof(float) * g.pitch * g.rows;
+    auto kern = lpaici_forward_kernel<P, WX, WY>;
+    int dev = 0, max_optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (smem > static_cast<size_t>(max_optin))
+        return set_error(LPAICI_ERR_UNSUPPORTED, "forward tile needs %zu B of shared memory, device allows %d", smem,
+                         max_optin);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute(forward)");
+    const dim3 grid((img.W + Shape::kTileW - 1) / Shape::kTileW, (img.rows_out + Shape::kTileH - 1) / Shape::kTileH);
+    if (grid.y > 65535u) return set_error(LPAICI_ERR_UNSUPPORTED, "image too tall: %d rows", img.rows_out);
+    kern<<<grid, Shape::kThreads, smem, stream>>>(img, tab);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_error(e, "forward launch");
+    return LPAICI_OK;
+}
+
+}  // namespace
+
+#define LPAICI_FWD_CASE(idx, P, WX, WY) \
+    case idx: return launch_cfg<P, WX, WY>(img, tab, stream);
+
+int launch_forward(const lpaici_kernelset *ks, const ImageArgs &img, const KernelTables &tab, int config,
+                   cudaStream_t stream) {
+    (void)ks;
+    switch (config) {
+        LPAICI_TILE_CONFIGS(LPAICI_FWD_CASE)
+        default: return set_error(LPAICI_ERR_INVALID_ARG, "tile config %d out of range", config);
+    }
+}
+
+}  // namespace lpaici

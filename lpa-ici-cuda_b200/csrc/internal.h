@@ -1,0 +1,96 @@
+// internal.h -- shared declarations of the LPA-ICI library (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "lpaici.h"
+
+namespace lpaici {
+
+// Limits of this build.  The per-kernel variance and threshold tables travel as kernel
+// parameters (2 * 4 B * kMaxKernels), so D*S is capped; the radius bounds the shared-memory halo.
+constexpr int kMaxKernels = 256;
+constexpr int kMaxRadius = 127;
+
+// One row run of a kernel, as the device reads it: the taps (dy, dx0 + j), j < len, with weights
+// weights[woff + j].  dy/dx0 are offsets from the output pixel (row - rows/2, col - cols/2).
+struct Run {
+    int dy, dx0, len, woff;
+};
+
+// Device image of a kernel set, one contiguous block of 32-bit words:
+//   [0, nk+1)                 first run of kernel k (kernel k's runs are [begin[k], begin[k+1]))
+//   [run_word, +4*n_runs)     Run records, 16-byte aligned
+//   [weight_word, +n_taps)    packed weights
+struct BlobLayout {
+    int nk = 0, n_runs = 0, n_taps = 0;
+    int run_word = 0, weight_word = 0, total_words = 0;  // total padded to a multiple of 4
+};
+
+// Per-launch arguments shared by the forward and backward kernels (passed by value as a
+// __grid_constant__ parameter; the tables are read with uniform indices from the constant bank).
+struct ImageArgs {
+    const float *in;  // input rows [0, in_h), width W, pitch in_pitch
+    float *out;       // output rows [0, rows_out), pitch out_pitch
+    const float *gout;  // backward only: cotangent, same geometry as out
+    uint8_t *smap;    // optional D x rows_out x W scale map
+    int W, in_h, in_pitch, out_pitch, gout_pitch;
+    int row_begin;    // output row r is input row row_begin + r
+    int rows_out;
+};
+
+struct KernelTables {
+    int D, S, R;
+    const int *blob;  // device blob (BlobLayout)
+    int blob_words, run_word, weight_word;
+    float var[kMaxKernels];
+    float thr[kMaxKernels];
+};
+
+int set_error(int code, const char *fmt, ...);
+int cuda_error(cudaError_t e, const char *what);
+
+}  // namespace lpaici
+
+// The opaque kernel set of the C ABI.
+struct lpaici_kernelset {
+    int D = 0, S = 0;
+    // the loader's dense output (load_LPA_kernels_standardized)
+    std::vector<float> dense_w;
+    std::vector<int> off, rows, cols;
+    // the reference-layout run packing (build_sparse_kernels)
+    std::vector<float> run_w;
+    std::vector<int> run_row, run_col, run_len, k_first_run, k_num_runs, k_first_weight;
+    // sum of squared weights per kernel, float, dense row-major order (compute_kernel_variances)
+    std::vector<float> norm2;
+    // nonzero taps per kernel (algorithmic work accounting)
+    std::vector<int> nnz;
+    int radius = 0;
+    lpaici::BlobLayout layout;
+    std::vector<int32_t> blob;  // host copy of the device blob
+    // device copies, one per CUDA device, created on first use
+    mutable std::mutex mu;
+    mutable std::vector<int *> dev_blob;
+    mutable std::vector<int> tuned_config;  // per device, -1 = not tuned
+};
+
+namespace lpaici {
+
+// Device blob of ks on the current device (uploaded on first use).  Returns an LPAICI_* code.
+int device_blob(const lpaici_kernelset *ks, const int **out);
+
+// Fills var/thr exactly as the reference: var = (sigma*sigma)*norm2, thr = gamma*sqrt(var).
+void fill_tables(const lpaici_kernelset *ks, const float *var_or_null, float sigma, float gamma, KernelTables *t);
+
+// Forward / backward launchers (forward.cu, backward.cu).
+int launch_forward(const lpaici_kernelset *ks, const ImageArgs &img, const KernelTables &tab, int config,
+                   cudaStream_t stream);
+int launch_backward(const lpaici_kernelset *ks, const ImageArgs &img, const KernelTables &tab, cudaStream_t stream);
+int default_config(const lpaici_kernelset *ks);
+
+}  // namespace lpaici

@@ -1,0 +1,428 @@
+// kernelset.cpp -- kernel-file loader, run-length packer, variances and the device kernel-set blob.
+//
+// Host code; built with -ffp-contract=off so every float multiply and add rounds separately, as in
+// the reference's x86-64 build (no FMA without -march).
+#include <cerrno>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <random>
+#include <sstream>
+
+#include "internal.h"
+
+namespace lpaici {
+
+static thread_local std::string g_last_error;
+
+int set_error(int code, const char *fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+int cuda_error(cudaError_t e, const char *what) {
+    return set_error(e == cudaErrorMemoryAllocation ? LPAICI_ERR_NO_MEMORY : LPAICI_ERR_CUDA, "%s: %s (%s)", what,
+                     cudaGetErrorString(e), cudaGetErrorName(e));
+}
+
+// ---------------------------------------------------------------------------------------------
+// Packing: one run per kernel row, from its first to its last nonzero (interior zeros kept), with
+// centre-relative coordinates (row - rows/2, first - cols/2): the layout of build_sparse_kernels
+// (src/v4_1_lpa_ici_2D_sparse_shared.cu:826-877), here without any capacity limit.
+// ---------------------------------------------------------------------------------------------
+static int finish_kernelset(lpaici_kernelset *ks) {
+    const int nk = ks->D * ks->S;
+    if (nk > kMaxKernels)
+        return set_error(LPAICI_ERR_UNSUPPORTED, "kernel set has %d kernels (%d directions x %d scales); at most %d",
+                         nk, ks->D, ks->S, kMaxKernels);
+    ks->norm2.assign(nk, 0.0f);
+    ks->nnz.assign(nk, 0);
+    ks->radius = 0;
+    for (int k = 0; k < nk; k++) {
+        const float *h = ks->dense_w.data() + ks->off[k];
+        const int R = ks->rows[k], Cc = ks->cols[k];
+        float nsq = 0.0f;
+        for (int i = 0; i < R * Cc; i++) nsq += h[i] * h[i];  // compute_kernel_variances order
+        ks->norm2[k] = nsq;
+        ks->k_first_run.push_back(static_cast<int>(ks->run_row.size()));
+        ks->k_first_weight.push_back(static_cast<int>(ks->run_w.size()));
+        for (int r = 0; r < R; r++) {
+            int first = -1, last = -1;
+            for (int c = 0; c < Cc; c++)
+                if (h[r * Cc + c] != 0.0f) {
+                    if (first < 0) first = c;
+                    last = c;
+                    ks->nnz[k]++;
+                }
+            if (first < 0) continue;
+            const int dy = r - R / 2, dx0 = first - Cc / 2, len = last - first + 1;
+            ks->run_row.push_back(dy);
+            ks->run_col.push_back(dx0);
+            ks->run_len.push_back(len);
+            for (int c = first; c <= last; c++) ks->run_w.push_back(h[r * Cc + c]);
+            int reach = std::abs(dy);
+            if (std::abs(dx0) > reach) reach = std::abs(dx0);
+            if (std::abs(dx0 + len - 1) > reach) reach = std::abs(dx0 + len - 1);
+            if (reach > ks->radius) ks->radius = reach;
+        }
+        ks->k_num_runs.push_back(static_cast<int>(ks->run_row.size()) - ks->k_first_run[k]);
+    }
+    if (ks->radius > kMaxRadius)
+        return set_error(LPAICI_ERR_UNSUPPORTED, "kernel radius %d exceeds the supported %d", ks->radius, kMaxRadius);
+
+    // device blob: [run begin per kernel (nk+1)] [Run records] [weights]
+    BlobLayout &L = ks->layout;
+    L.nk = nk;
+    L.n_runs = static_cast<int>(ks->run_row.size());
+    L.n_taps = static_cast<int>(ks->run_w.size());
+    L.run_word = (nk + 1 + 3) & ~3;
+    L.weight_word = L.run_word + 4 * L.n_runs;
+    L.total_words = (L.weight_word + L.n_taps + 3) & ~3;
+    ks->blob.assign(L.total_words, 0);
+    for (int k = 0; k < nk; k++) ks->blob[k] = ks->k_first_run[k];
+    ks->blob[nk] = L.n_runs;
+    for (int r = 0; r < L.n_runs; r++) {
+        ks->blob[L.run_word + 4 * r + 0] = ks->run_row[r];
+        ks->blob[L.run_word + 4 * r + 1] = ks->run_col[r];
+        ks->blob[L.run_word + 4 * r + 2] = ks->run_len[r];
+        ks->blob[L.run_word + 4 * r + 3] = 0;
+    }
+    // woff: index of the run's first weight; runs are packed back to back per kernel
+    for (int k = 0; k < nk; k++) {
+        int w = ks->k_first_weight[k];
+        for (int r = ks->k_first_run[k]; r < ks->k_first_run[k] + ks->k_num_runs[k]; r++) {
+            ks->blob[L.run_word + 4 * r + 3] = w;
+            w += ks->run_len[r];
+        }
+    }
+    std::memcpy(ks->blob.data() + L.weight_word, ks->run_w.data(), sizeof(float) * L.n_taps);
+    return LPAICI_OK;
+}
+
+int device_blob(const lpaici_kernelset *ks, const int **out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_error(e, "cudaGetDevice");
+    std::lock_guard<std::mutex> lock(ks->mu);
+    if (static_cast<int>(ks->dev_blob.size()) <= dev) {
+        ks->dev_blob.resize(dev + 1, nullptr);
+        ks->tuned_config.resize(dev + 1, -1);
+    }
+    if (!ks->dev_blob[dev]) {
+        int *p = nullptr;
+        e = cudaMalloc(&p, sizeof(int32_t) * ks->blob.size());
+        if (e != cudaSuccess) return cuda_error(e, "cudaMalloc(kernel set)");
+        e = cudaMemcpy(p, ks->blob.data(), sizeof(int32_t) * ks->blob.size(), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            cudaFree(p);
+            return cuda_error(e, "cudaMemcpy(kernel set)");
+        }
+        ks->dev_blob[dev] = p;
+    }
+    *out = ks->dev_blob[dev];
+    return LPAICI_OK;
+}
+
+void fill_tables(const lpaici_kernelset *ks, const float *var_or_null, float sigma, float gamma, KernelTables *t) {
+    const int nk = ks->D * ks->S;
+    t->D = ks->D;
+    t->S = ks->S;
+    t->R = ks->radius;
+    t->blob_words = ks->layout.total_words;
+    t->run_word = ks->layout.run_word;
+    t->weight_word = ks->layout.weight_word;
+    const float s2 = sigma * sigma;
+    for (int k = 0; k < nk; k++) {
+        const float v = var_or_null ? var_or_null[k] : s2 * ks->norm2[k];
+        t->var[k] = v;
+        t->thr[k] = gamma * std::sqrt(v);  // src/v1_0_lpa_ici_2D_fused.cpp:905
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Text loader with the semantics of load_LPA_kernels_standardized
+// (src/v1_0_lpa_ici_2D_fused.cpp:466-551): header "D S" (> 0), then per kernel "rows cols" (> 0)
+// and rows*cols weights; direction 0 fixes each scale's size; every other direction is
+// centre-cropped to it with offset (file - target) / 2.
+// ---------------------------------------------------------------------------------------------
+namespace {
+// Numbers are read like std::istream's operator>> in the "C" locale: skip whitespace, take the
+// longest prefix that looks like a number and leave the rest of the text for the next read.
+//   int:   [+-]?[0-9]+                                    (fails on overflow)
+//   float: [+-]?[0-9]*(\.[0-9]*)?([eE][+-]?[0-9]*)?  with at least one mantissa digit, converted
+//          with correct rounding (strtof); fails if the exponent has no digits or the value
+//          overflows; underflow gives 0 or a subnormal.  "inf", "nan" and hex text fail or stop at
+//          the first letter, as they do for operator>>.
+struct Stream {
+    const char *p, *end;
+    static bool space(char c) { return c == ' ' || c == '\n' || c == '\t' || c == '\r' || c == '\v' || c == '\f'; }
+    static bool digit(char c) { return c >= '0' && c <= '9'; }
+    void skip() {
+        while (p < end && space(*p)) p++;
+    }
+    bool next_int(int &v) {
+        skip();
+        const char *b = p;
+        if (p < end && (*p == '+' || *p == '-')) p++;
+        const char *d = p;
+        while (p < end && digit(*p)) p++;
+        if (p == d) return false;
+        const std::string t(b, p);
+        errno = 0;
+        const long x = std::strtol(t.c_str(), nullptr, 10);
+        if (errno != 0 || x > 2147483647L || x < -2147483647L - 1) return false;
+        v = static_cast<int>(x);
+        return true;
+    }
+    bool next_float(float &v) {
+        skip();
+        const char *b = p;
+        if (p < end && (*p == '+' || *p == '-')) p++;
+        int mant = 0;
+        while (p < end && digit(*p)) p++, mant++;
+        if (p < end && *p == '.') {
+            p++;
+            while (p < end && digit(*p)) p++, mant++;
+        }
+        if (mant == 0) return false;
+        if (p < end && (*p == 'e' || *p == 'E')) {
+            p++;
+            if (p < end && (*p == '+' || *p == '-')) p++;
+            int ed = 0;
+            while (p < end && digit(*p)) p++, ed++;
+            if (ed == 0) return false;
+        }
+        const std::string t(b, p);
+        char *e = nullptr;
+        v = std::strtof(t.c_str(), &e);
+        return *e == '\0' && !std::isinf(v);
+    }
+};
+}  // namespace
+
+}  // namespace lpaici
+
+using namespace lpaici;
+
+extern "C" {
+
+const char *lpaici_last_error(void) { return g_last_error.c_str(); }
+
+const char *lpaici_status_string(int status) {
+    switch (status) {
+        case LPAICI_OK: return "LPAICI_OK";
+        case LPAICI_ERR_INVALID_ARG: return "LPAICI_ERR_INVALID_ARG";
+        case LPAICI_ERR_FILE: return "LPAICI_ERR_FILE";
+        case LPAICI_ERR_KERNEL_FORMAT: return "LPAICI_ERR_KERNEL_FORMAT";
+        case LPAICI_ERR_UNSUPPORTED: return "LPAICI_ERR_UNSUPPORTED";
+        case LPAICI_ERR_CUDA: return "LPAICI_ERR_CUDA";
+        case LPAICI_ERR_NO_MEMORY: return "LPAICI_ERR_NO_MEMORY";
+        default: return "LPAICI_ERR_UNKNOWN";
+    }
+}
+
+int lpaici_kernelset_load(const char *path, lpaici_kernelset **out) {
+    if (!path || !out) return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_kernelset_load: null argument");
+    *out = nullptr;
+    std::ifstream f(path, std::ios::binary);
+    if (!f.is_open()) return set_error(LPAICI_ERR_FILE, "Failed to open %s", path);
+    std::stringstream ss;
+    ss << f.rdbuf();
+    const std::string text = ss.str();
+    Stream tk{text.data(), text.data() + text.size()};
+
+    int D = 0, S = 0;
+    if (!tk.next_int(D) || !tk.next_int(S) || D <= 0 || S <= 0)
+        return set_error(LPAICI_ERR_KERNEL_FORMAT, "invalid header in %s", path);
+    if (static_cast<long>(D) * S > kMaxKernels)
+        return set_error(LPAICI_ERR_UNSUPPORTED, "%s has %d x %d kernels; at most %d", path, D, S, kMaxKernels);
+
+    auto *ks = new lpaici_kernelset();
+    ks->D = D;
+    ks->S = S;
+    std::vector<int> trow(S), tcol(S);
+    std::vector<float> tmp;
+    for (int d = 0; d < D; d++) {
+        for (int s = 0; s < S; s++) {
+            int fr = 0, fc = 0;
+            if (!tk.next_int(fr) || !tk.next_int(fc) || fr <= 0 || fc <= 0 || static_cast<long>(fr) * fc > (1L << 26)) {
+                delete ks;
+                return set_error(LPAICI_ERR_KERNEL_FORMAT, "invalid size of kernel %d, %d in %s", d, s, path);
+            }
+            tmp.resize(static_cast<size_t>(fr) * fc);
+            for (auto &v : tmp)
+                if (!tk.next_float(v)) {
+                    delete ks;
+                    return set_error(LPAICI_ERR_KERNEL_FORMAT, "missing weights of kernel %d, %d in %s", d, s, path);
+                }
+            if (d == 0) {
+                trow[s] = fr;
+                tcol[s] = fc;
+            }
+            const int tr = trow[s], tc = tcol[s];
+            if (fr < tr || fc < tc) {
+                delete ks;
+                return set_error(LPAICI_ERR_KERNEL_FORMAT,
+                                 "Matrix at direction %d, scale %d is too small to crop to the target size", d, s);
+            }
+            const int ro = (fr - tr) / 2, co = (fc - tc) / 2;
+            ks->off.push_back(static_cast<int>(ks->dense_w.size()));
+            ks->rows.push_back(tr);
+            ks->cols.push_back(tc);
+            for (int r = 0; r < tr; r++)
+                for (int c = 0; c < tc; c++) ks->dense_w.push_back(tmp[static_cast<size_t>(r + ro) * fc + (c + co)]);
+        }
+    }
+    int rc = finish_kernelset(ks);
+    if (rc != LPAICI_OK) {
+        delete ks;
+        return rc;
+    }
+    // best effort: upload to the current device now, outside any stream capture
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) == cudaSuccess && ndev > 0) {
+        const int *p = nullptr;
+        rc = device_blob(ks, &p);
+        if (rc != LPAICI_OK) {
+            delete ks;
+            return rc;
+        }
+    } else {
+        cudaGetLastError();
+    }
+    *out = ks;
+    return LPAICI_OK;
+}
+
+int lpaici_kernelset_create(const float *weights, const int *offsets, const int *rows, const int *cols, int num_dirs,
+                            int num_scales, lpaici_kernelset **out) {
+    if (!weights || !offsets || !rows || !cols || !out || num_dirs <= 0 || num_scales <= 0)
+        return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_kernelset_create: null array or non-positive D/S");
+    *out = nullptr;
+    const long nk = static_cast<long>(num_dirs) * num_scales;
+    if (nk > kMaxKernels)
+        return set_error(LPAICI_ERR_UNSUPPORTED, "%d x %d kernels; at most %d", num_dirs, num_scales, kMaxKernels);
+    auto *ks = new lpaici_kernelset();
+    ks->D = num_dirs;
+    ks->S = num_scales;
+    for (long k = 0; k < nk; k++) {
+        if (rows[k] <= 0 || cols[k] <= 0 || offsets[k] < 0 || static_cast<long>(rows[k]) * cols[k] > (1L << 26)) {
+            delete ks;
+            return set_error(LPAICI_ERR_KERNEL_FORMAT, "kernel %ld has size %d x %d at offset %d", k, rows[k], cols[k],
+                             offsets[k]);
+        }
+        ks->off.push_back(static_cast<int>(ks->dense_w.size()));
+        ks->rows.push_back(rows[k]);
+        ks->cols.push_back(cols[k]);
+        ks->dense_w.insert(ks->dense_w.end(), weights + offsets[k], weights + offsets[k] + rows[k] * cols[k]);
+    }
+    int rc = finish_kernelset(ks);
+    if (rc != LPAICI_OK) {
+        delete ks;
+        return rc;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) == cudaSuccess && ndev > 0) {
+        const int *p = nullptr;
+        rc = device_blob(ks, &p);
+        if (rc != LPAICI_OK) {
+            delete ks;
+            return rc;
+        }
+    } else {
+        cudaGetLastError();
+    }
+    *out = ks;
+    return LPAICI_OK;
+}
+
+int lpaici_kernelset_destroy(lpaici_kernelset *ks) {
+    if (!ks) return LPAICI_OK;
+    int cur = -1;
+    cudaGetDevice(&cur);
+    for (size_t d = 0; d < ks->dev_blob.size(); d++)
+        if (ks->dev_blob[d]) {
+            cudaSetDevice(static_cast<int>(d));
+            cudaFree(ks->dev_blob[d]);
+        }
+    if (cur >= 0) cudaSetDevice(cur);
+    cudaGetLastError();
+    delete ks;
+    return LPAICI_OK;
+}
+
+int lpaici_kernelset_get_info(const lpaici_kernelset *ks, lpaici_kernelset_info_t *info) {
+    if (!ks || !info) return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_kernelset_get_info: null argument");
+    info->num_dirs = ks->D;
+    info->num_scales = ks->S;
+    info->dense_size = static_cast<int>(ks->dense_w.size());
+    info->n_taps = static_cast<int>(ks->run_w.size());
+    info->n_runs = static_cast<int>(ks->run_row.size());
+    info->radius = ks->radius;
+    return LPAICI_OK;
+}
+
+int lpaici_kernelset_get_dense(const lpaici_kernelset *ks, float *weights, int *offsets, int *rows, int *cols) {
+    if (!ks || !weights || !offsets || !rows || !cols)
+        return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_kernelset_get_dense: null argument");
+    std::memcpy(weights, ks->dense_w.data(), sizeof(float) * ks->dense_w.size());
+    std::memcpy(offsets, ks->off.data(), sizeof(int) * ks->off.size());
+    std::memcpy(rows, ks->rows.data(), sizeof(int) * ks->rows.size());
+    std::memcpy(cols, ks->cols.data(), sizeof(int) * ks->cols.size());
+    return LPAICI_OK;
+}
+
+int lpaici_kernelset_get_runs(const lpaici_kernelset *ks, float *weights, int *run_row, int *run_col, int *run_len,
+                              int *kernel_first_run, int *kernel_num_runs, int *kernel_first_weight) {
+    if (!ks || !weights || !run_row || !run_col || !run_len || !kernel_first_run || !kernel_num_runs ||
+        !kernel_first_weight)
+        return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_kernelset_get_runs: null argument");
+    std::memcpy(weights, ks->run_w.data(), sizeof(float) * ks->run_w.size());
+    std::memcpy(run_row, ks->run_row.data(), sizeof(int) * ks->run_row.size());
+    std::memcpy(run_col, ks->run_col.data(), sizeof(int) * ks->run_col.size());
+    std::memcpy(run_len, ks->run_len.data(), sizeof(int) * ks->run_len.size());
+    std::memcpy(kernel_first_run, ks->k_first_run.data(), sizeof(int) * ks->k_first_run.size());
+    std::memcpy(kernel_num_runs, ks->k_num_runs.data(), sizeof(int) * ks->k_num_runs.size());
+    std::memcpy(kernel_first_weight, ks->k_first_weight.data(), sizeof(int) * ks->k_first_weight.size());
+    return LPAICI_OK;
+}
+
+int lpaici_kernel_variances(const lpaici_kernelset *ks, float sigma, float *var) {
+    if (!ks || !var) return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_kernel_variances: null argument");
+    const float s2 = sigma * sigma;
+    for (int k = 0; k < ks->D * ks->S; k++) var[k] = s2 * ks->norm2[k];
+    return LPAICI_OK;
+}
+
+int lpaici_add_noise(const float *clean, float *noisy, long n, float sigma, unsigned int seed) {
+    if (!clean || !noisy || n < 0) return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_add_noise: bad argument");
+    std::mt19937 gen{seed};
+    std::normal_distribution<float> dist{0.0, sigma};
+    for (long i = 0; i < n; i++) {
+        const float sample = dist(gen);
+        noisy[i] = clean[i] + sample;
+    }
+    return LPAICI_OK;
+}
+
+double lpaici_psnr(const float *a, const float *b, long n) {
+    if (!a || !b || n <= 0) return NAN;
+    double sum = 0.0;
+    for (long i = 0; i < n; i++) {
+        const float diff = a[i] - b[i];
+        const float sq = diff * diff;
+        sum += sq;
+    }
+    const double mse = sum / n;
+    return 10.0 * std::log10(1.0f / mse);
+}
+
+}  // extern "C"

@@ -1,0 +1,101 @@
+"""Adjoint (selection frozen): the CUDA backward against the FP64 oracle's adjoint and against central
+finite differences (eps = 1e-3) of the frozen-selection map in the FP64 oracle.  The gradcheck harness
+wraps forward/backward in a torch.autograd.Function (test code only).
+
+Tolerance: the kernel accumulates in FP32 (FMA, atomics in any order); the FP64 references are exact to
+~1e-12.  We require |grad - ref| <= 2e-5 * max|ref| + 1e-6 everywhere (an FP32 sum of a few thousand
+terms of magnitude <= max|ref| carries a relative error of order 1e-6)."""
+import numpy as np
+import pytest
+
+import lpaici
+import oracle_bind as ob
+from conftest import GAUSS_M2, SYM, kernel_file
+
+pytestmark = pytest.mark.gpu
+SIGMA_20 = float(np.float32(20.0) / np.float32(255.0))
+RTOL = 2e-5
+
+
+class LpaIci:
+    """torch.autograd.Function over the C ABI: forward = lpaici_forward, backward = lpaici_backward."""
+
+    @staticmethod
+    def make(ks, sigma, gamma):
+        import torch
+
+        class Fn(torch.autograd.Function):
+            @staticmethod
+            def forward(ctx, x):
+                ctx.save_for_backward(x)
+                return lpaici.forward(ks, x.contiguous(), sigma, gamma)
+
+            @staticmethod
+            def backward(ctx, g):
+                (x,) = ctx.saved_tensors
+                return lpaici.backward(ks, x.contiguous(), g.contiguous(), sigma, gamma)
+
+        return Fn.apply
+
+
+def _case(name, W, H, sigma, gamma, seed):
+    import torch
+
+    ks = lpaici.KernelSet.load(kernel_file(name))
+    ko = ob.oracle_load_kernels(kernel_file(name))
+    noisy = lpaici.add_noise(lpaici.synth_image(W, H, seed), sigma, 20250910 + seed)
+    g = np.random.default_rng(seed).standard_normal((H, W)).astype(np.float32)
+    xt = torch.from_numpy(noisy).cuda()
+    gt = torch.from_numpy(g).cuda()
+    grad = lpaici.backward(ks, xt, gt, sigma, gamma).cpu().numpy()
+    var = ks.variances(sigma)
+    _, smap, _ = ob.oracle_forward_f32(noisy, ko, var, gamma, want_map=True)
+    return ks, ko, noisy, g, grad, var, smap
+
+
+@pytest.mark.parametrize("name,W,H,sigma,gamma,seed", [
+    (SYM, 64, 48, SIGMA_20, 2.0, 1), (SYM, 130, 37, SIGMA_20, 2.0, 2), (SYM, 1, 1, SIGMA_20, 2.0, 3),
+    (SYM, 97, 5, SIGMA_20, 1.5, 4), (GAUSS_M2, 80, 72, float(np.float32(25.0) / np.float32(255.0)), 1.5, 5),
+])
+def test_backward_vs_fp64_adjoint(name, W, H, sigma, gamma, seed):
+    ks, ko, noisy, g, grad, var, smap = _case(name, W, H, sigma, gamma, seed)
+    ref = ob.oracle_adjoint_f64(ko, var, smap, g.astype(np.float64))
+    err = np.abs(grad - ref).max()
+    assert err <= RTOL * np.abs(ref).max() + 1e-6, (err, np.abs(ref).max())
+
+
+def test_backward_vs_central_differences():
+    """Config of the adjoint check, scaled to test time: 256 random pixels, eps = 1e-3, FP64 oracle."""
+    ks, ko, noisy, g, grad, var, smap = _case(SYM, 256, 256, SIGMA_20, 2.0, 7)
+    rng = np.random.default_rng(11)
+    q = rng.choice(noisy.size, size=256, replace=False).astype(np.int64)
+    fd = ob.oracle_fd_grad_f64(noisy, ko, var, smap, g.astype(np.float64), q, 1e-3)
+    got = grad.ravel()[q]
+    err = np.abs(got - fd).max()
+    assert err <= RTOL * np.abs(fd).max() + 1e-6, (err, np.abs(fd).max())
+
+
+def test_autograd_harness():
+    import torch
+
+    ks, ko, noisy, g, grad, var, smap = _case(SYM, 96, 80, SIGMA_20, 2.0, 9)
+    f = LpaIci.make(ks, SIGMA_20, 2.0)
+    x = torch.from_numpy(noisy).cuda().requires_grad_(True)
+    w = torch.from_numpy(g).cuda()
+    loss = (w * f(x)).sum()
+    loss.backward()
+    q = np.random.default_rng(3).choice(noisy.size, size=64, replace=False).astype(np.int64)
+    fd = ob.oracle_fd_grad_f64(noisy, ko, var, smap, g.astype(np.float64), q, 1e-3)
+    got = x.grad.cpu().numpy().ravel()[q]
+    assert np.abs(got - fd).max() <= RTOL * np.abs(fd).max() + 1e-6
+    # atomics make the summation order vary between runs: equal to the direct call up to FP32 rounding
+    assert np.abs(x.grad.cpu().numpy() - grad).max() <= RTOL * np.abs(grad).max() + 1e-6
+
+
+def test_backward_errors():
+    import torch
+
+    ks = lpaici.KernelSet.load(kernel_file(SYM))
+    x = torch.zeros((4, 4), device="cuda")
+    with pytest.raises(lpaici.LpaIciError):
+        lpaici.backward(ks, x, x, -1.0, 2.0)

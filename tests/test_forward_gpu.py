@@ -1,0 +1,185 @@
+"""Parity of the CUDA forward (through the C ABI) with the reference: bit-exact output and scale maps.
+
+Small cases compare with the committed golden outputs (made by the reference's own
+anisotropic_lpa_ici_cpu_fused) and with the oracle; barbara must reproduce the reference's denoised
+image bit for bit (hash) and its published PSNRs; the 4096^2 benchmark image is checked exactly on
+random windows against the oracle run on the window plus its 31-pixel halo.
+"""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import lpaici
+import oracle_bind as ob
+from conftest import GOLDEN, SYM, kernel_file
+
+pytestmark = pytest.mark.gpu
+
+CASES = json.load(open(os.path.join(GOLDEN, "forward_cases.json")))
+ARR = np.load(os.path.join(GOLDEN, "forward_cases.npz"))
+SIGMA_20 = float(np.float32(20.0) / np.float32(255.0))
+
+
+def bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch
+
+    assert torch.cuda.is_available()
+    return torch
+
+
+_ks_cache = {}
+
+
+def ks_for(name):
+    if name not in _ks_cache:
+        _ks_cache[name] = (lpaici.KernelSet.load(kernel_file(name)), ob.oracle_load_kernels(kernel_file(name)))
+    return _ks_cache[name]
+
+
+def gpu_forward(torch, ks, x, sigma, gamma, smap=False, **kw):
+    t = torch.from_numpy(np.ascontiguousarray(x, np.float32)).cuda()
+    r = lpaici.forward(ks, t, sigma, gamma, scale_map=smap, **kw)
+    torch.cuda.synchronize()
+    if smap:
+        return r[0].cpu().numpy(), r[1].cpu().numpy()
+    return r.cpu().numpy()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_golden_cases_bit_exact(torch, name):
+    ks, ko = ks_for(CASES[name]["kernels"])
+    sigma, gamma = (float(v) for v in ARR[f"{name}/params"])
+    noisy = ARR[f"{name}/noisy"]
+    out, smap = gpu_forward(torch, ks, noisy, sigma, gamma, smap=True)
+    assert np.array_equal(bits(out), bits(ARR[f"{name}/out"]))
+    _, osmap, _ = ob.oracle_forward_f32(noisy, ko, ARR[f"{name}/var"], gamma, want_map=True)
+    assert np.array_equal(smap, osmap)
+    assert lpaici.psnr(ARR[f"{name}/clean"], out) == ARR[f"{name}/psnr"][1]
+
+
+@pytest.mark.parametrize("name", ["sym_64x48", "gauss_m2_80x72", "tapered_72x40"])
+def test_caller_variances_path(torch, name):
+    """lpaici_forward_var: the reference engine's convention (variances computed by the caller)."""
+    ks, _ = ks_for(CASES[name]["kernels"])
+    gamma = float(ARR[f"{name}/params"][1])
+    out = gpu_forward(torch, ks, ARR[f"{name}/noisy"], 0.0, gamma, variances=ARR[f"{name}/var"])
+    assert np.array_equal(bits(out), bits(ARR[f"{name}/out"]))
+
+
+@pytest.mark.parametrize("config", range(lpaici.lib().lpaici_num_tile_configs()))
+def test_every_tile_config(torch, config):
+    ks, ko = ks_for(SYM)
+    try:
+        ks.set_tile_config(config)
+        for W, H, seed in ((130, 37, 1), (211, 150, 2), (33, 9, 3)):
+            clean = lpaici.synth_image(W, H, seed)
+            noisy = lpaici.add_noise(clean, SIGMA_20, 20250910 + seed)
+            out, smap = gpu_forward(torch, ks, noisy, SIGMA_20, 2.0, smap=True)
+            ref, osmap, _ = ob.oracle_forward_f32(noisy, ko, ks.variances(SIGMA_20), 2.0, want_map=True)
+            assert np.array_equal(bits(out), bits(ref)), (W, H)
+            assert np.array_equal(smap, osmap), (W, H)
+    finally:
+        ks.set_tile_config(-1)
+
+
+def test_pitched_buffers(torch):
+    ks, ko = ks_for(SYM)
+    W, H = 150, 70
+    noisy = lpaici.add_noise(lpaici.synth_image(W, H, 5), SIGMA_20, 7)
+    big_in = torch.full((H, W + 37), float("nan"), device="cuda")
+    big_in[:, :W] = torch.from_numpy(noisy).cuda()
+    big_out = torch.full((H, W + 11), -5.0, device="cuda")
+    lpaici.forward(ks, big_in[:, :W], SIGMA_20, 2.0, out=big_out[:, :W])
+    torch.cuda.synchronize()
+    ref, _, _ = ob.oracle_forward_f32(noisy, ko, ks.variances(SIGMA_20), 2.0)
+    got = big_out.cpu().numpy()
+    assert np.array_equal(bits(got[:, :W]), bits(ref))
+    assert np.all(got[:, W:] == -5.0)  # nothing written beyond the width
+
+
+def test_barbara_reproduces_reference(torch):
+    """The reference's own result on data/barbara.png (defaults): same denoised bits, same PSNRs
+    (published 22.1056 / 25.0736 dB, readme.md:7)."""
+    meta = json.load(open(os.path.join(GOLDEN, "barbara.json")))
+    u8 = np.load(os.path.join(GOLDEN, "barbara_gray_u8.npy"))
+    lut = (np.power((np.arange(256, dtype=np.float32) / np.float32(255.0)).astype(np.float64),
+                    np.float64(np.float32(2.2))) * 1.0).astype(np.float32)
+    clean = lut[u8]
+    noisy = lpaici.add_noise(clean, SIGMA_20, 20250910)
+    ks, _ = ks_for(SYM)
+    out = gpu_forward(torch, ks, noisy, SIGMA_20, 2.0)
+    assert hashlib.sha256(out.tobytes()).hexdigest() == meta["denoised_sha256"]
+    assert lpaici.psnr(clean, noisy) == meta["psnr_noisy"]
+    assert lpaici.psnr(clean, out) == meta["psnr_denoised"]
+    assert round(meta["psnr_denoised"], 4) == meta["published_psnr_denoised"]
+
+
+def test_reference_engine_signature(torch):
+    """lpaici_anisotropic_gpu_fused: host buffers, dense kernels and caller variances, like the
+    reference's anisotropic_lpa_ici_gpu_fused."""
+    name = "sym_130x37"
+    ks, _ = ks_for(SYM)
+    w, o, r, c = ks.dense()
+    out, secs = lpaici.anisotropic_gpu_fused(ARR[f"{name}/noisy"], w, o, r, c, 16, 7, ARR[f"{name}/var"], 2.0)
+    assert np.array_equal(bits(out), bits(ARR[f"{name}/out"]))
+    assert secs > 0
+    out2 = lpaici.denoise_host(ks, ARR[f"{name}/noisy"], SIGMA_20, 2.0)
+    assert np.array_equal(bits(out2), bits(ARR[f"{name}/out"]))
+
+
+def test_row_bands_reproduce_full_image(torch):
+    """Splitting an image into row bands with a radius-row halo (the multi-GPU decomposition) gives
+    exactly the full-image result."""
+    ks, _ = ks_for(SYM)
+    W, H, R = 300, 257, ks.radius
+    noisy = torch.from_numpy(lpaici.add_noise(lpaici.synth_image(W, H, 9), SIGMA_20, 3)).cuda()
+    full = lpaici.forward(ks, noisy, SIGMA_20, 2.0)
+    pieces = []
+    for b0, b1 in ((0, 64), (64, 100), (100, 257)):
+        lo, hi = max(0, b0 - R), min(H, b1 + R)
+        pieces.append(lpaici.forward_rows(ks, noisy[lo:hi], b0 - lo, b1 - b0, SIGMA_20, 2.0))
+    torch.cuda.synchronize()
+    assert torch.equal(torch.cat(pieces).view(torch.int32), full.view(torch.int32))
+
+
+@pytest.mark.slow
+def test_4096_windows_exact(torch):
+    """The benchmark workload (4096^2 synthetic, sym 16x7, sigma 20/255, gamma 2): output and scale
+    maps equal the oracle's on 6 random 64x64 windows (oracle run on window + 31 px halo)."""
+    ks, ko = ks_for(SYM)
+    N, R = 4096, 31
+    clean = lpaici.synth_image(N, N, 20250910)
+    noisy = lpaici.add_noise(clean, SIGMA_20, 20250910)
+    out, smap = gpu_forward(torch, ks, noisy, SIGMA_20, 2.0, smap=True)
+    var = ks.variances(SIGMA_20)
+    rng = np.random.default_rng(0)
+    corners = [(0, 0), (N - 64, N - 64)] + [tuple(rng.integers(0, N - 64, 2)) for _ in range(4)]
+    for y, x in corners:
+        y0, x0, y1, x1 = max(0, y - R), max(0, x - R), min(N, y + 64 + R), min(N, x + 64 + R)
+        ref, rsmap, _ = ob.oracle_forward_f32(noisy[y0:y1, x0:x1], ko, var, 2.0, want_map=True)
+        assert np.array_equal(bits(out[y:y + 64, x:x + 64]), bits(ref[y - y0:y - y0 + 64, x - x0:x - x0 + 64]))
+        assert np.array_equal(smap[:, y:y + 64, x:x + 64], rsmap[:, y - y0:y - y0 + 64, x - x0:x - x0 + 64])
+    assert np.isfinite(out).all() and smap.max() < 7
+
+
+def test_invalid_arguments(torch):
+    ks, _ = ks_for(SYM)
+    x = torch.zeros((8, 8), device="cuda")
+    for sigma, gamma in ((0.0, 2.0), (-1.0, 2.0), (0.1, 0.0), (0.1, float("nan")), (float("inf"), 2.0)):
+        with pytest.raises(lpaici.LpaIciError) as e:
+            lpaici.forward(ks, x, sigma, gamma)
+        assert e.value.code == lpaici.ERR_INVALID_ARG
+    lib = lpaici.lib()
+    assert lib.lpaici_forward(ks.handle, None, 8, None, 8, 8, 8, 0.1, 2.0, None, None) == lpaici.ERR_INVALID_ARG
+    assert lib.lpaici_forward(ks.handle, x.data_ptr(), 4, x.data_ptr(), 8, 8, 8, 0.1, 2.0, None,
+                              None) == lpaici.ERR_INVALID_ARG
+    assert lib.lpaici_forward(None, x.data_ptr(), 8, x.data_ptr(), 8, 8, 8, 0.1, 2.0, None,
+                              None) == lpaici.ERR_INVALID_ARG
