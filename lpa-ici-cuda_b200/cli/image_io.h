@@ -1,0 +1,26 @@
+// image_io.h -- the image formats the drop-in command line reads and writes.
+//
+// Loading returns the gray float image the reference gets from stb_image's stbi_loadf(path, .., 1)
+// (src/v4_1_lpa_ici_2D_sparse_shared.cu:375):
+//   * PNG (8-bit or 16-bit, gray / gray+alpha / RGB / RGBA / palette, bit depths 1-16, interlaced or
+//     not): 16-bit samples keep their high byte, RGB becomes (77 R + 150 G + 29 B) >> 8, then every
+//     8-bit value v becomes (float) pow(v / 255.0f, 2.2f) -- stb's LDR-to-HDR conversion;
+//   * Radiance .hdr (RGBE, flat or run-length scanlines): gray = (R + G + B) * 2^(E - 136) / 3;
+//   * binary PGM (P5, 8-bit), converted like 8-bit PNG gray.
+// Writing produces a Radiance .hdr (RGBE, run-length scanlines for widths 8..32767), gray stored as
+// R = G = B, as stbi_write_hdr does for one channel (src/v4_1_lpa_ici_2D_sparse_shared.cu:388, :522).
+#pragma once
+
+#include <string>
+#include <vector>
+
+namespace lpaici_cli {
+
+// Returns false and sets err on failure.
+bool load_gray(const std::string &path, std::vector<float> &img, int &width, int &height, std::string &err);
+bool write_hdr(const std::string &path, const float *img, int width, int height);
+
+// The 256 values of stb's 8-bit to float conversion (pow(v/255, 2.2)).
+const float *ldr_to_float_table();
+
+}  // namespace lpaici_cli
