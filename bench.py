@@ -256,13 +256,18 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     torch.cuda.set_device(dev)
     tmp = tempfile.mkdtemp()
     ks = lpaici.KernelSet.load(kernel_path(SYM, tmp))
-    clean, noisy_h = bench_image(SIZE, SEED + rank, SIGMA)
+    size = args.size
+    clean, noisy_h = bench_image(size, SEED + rank, SIGMA)
     x = torch.from_numpy(noisy_h).to(dev)
     out = torch.empty_like(x)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
 
     # untimed: tile autotune on this image, scale maps for the algorithmic tap count
-    best, tune_ms = ks.autotune(SIZE, SIZE, SIGMA, GAMMA, sample=x, reps=2)
+    if args.tile_config >= 0:
+        best, tune_ms = args.tile_config, []
+        ks.set_tile_config(best)
+    else:
+        best, tune_ms = ks.autotune(size, size, SIGMA, GAMMA, sample=x, reps=2)
     _, smap = lpaici.forward(ks, x, SIGMA, GAMMA, out=out, scale_map=True)
     torch.cuda.synchronize()
     taps = algorithmic_taps(torch, ks, smap)
@@ -289,7 +294,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         t = torch.tensor([ms_step], device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms_step = float(t.item())
-    px = SIZE * SIZE
+    px = size * size
     value = world * px / (ms_step * 1e-3) / 1e6
 
     # parity of this run: two windows against the oracle (window + 31 px halo), bit for bit
@@ -344,7 +349,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "plain LPA-ICI forward, one 4096x4096 synthetic image per GPU, sym 16x7 kernels, "
+        "config": {"workload": f"plain LPA-ICI forward, one {size}x{size} synthetic image per GPU, sym 16x7 kernels, "
                                "sigma 20/255, gamma 2",
                    "image": "polygons + linear ramp + 4-16 px stripes, RGBE-quantised, seed 20250910 (+rank)",
                    "l2": "flushed between timed steps (256 MB write)",
@@ -384,8 +389,9 @@ def check_windows(torch, ks, noisy_h, out, rank):
     got = out.cpu().numpy()
     R, n, ok = ks.radius, 48, True
     rng = np.random.default_rng(rank)
-    for y, x in [(0, 0)] + [tuple(int(v) for v in rng.integers(0, SIZE - n, 2))]:
-        y0, x0, y1, x1 = max(0, y - R), max(0, x - R), min(SIZE, y + n + R), min(SIZE, x + n + R)
+    H, W = noisy_h.shape
+    for y, x in [(0, 0)] + [tuple(int(v) for v in rng.integers(0, min(H, W) - n, 2))]:
+        y0, x0, y1, x1 = max(0, y - R), max(0, x - R), min(H, y + n + R), min(W, x + n + R)
         ref, _, _ = ob.oracle_forward_f32(noisy_h[y0:y1, x0:x1], ko, var, GAMMA)
         ok &= np.array_equal(got[y:y + n, x:x + n].view(np.uint32),
                              ref[y - y0:y - y0 + n, x - x0:x - x0 + n].view(np.uint32))
@@ -462,6 +468,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-parity", action="store_true")
+    ap.add_argument("--size", type=int, default=SIZE, help="image side (profiling runs use a smaller case)")
+    ap.add_argument("--tile-config", type=int, default=-1, help="fixed tile configuration instead of autotuning")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
