@@ -10,7 +10,8 @@
 //   2. scatter: the input tile's shared memory becomes a gradient tile (tile + halo R); for every
 //      direction and every scale present in the warp, each thread spreads c_i = g_i * alpha_{d,i}
 //      (zero for pixels that selected another scale) through the kernel's row runs with a sliding
-//      window of P partial outputs: P FMAs per weight, one shared-memory atomic per finished output;
+//      window of 4 partial outputs per pixel row: 4 FMAs per weight, one shared-memory atomic per
+//      finished output;
 //   3. write-back: the gradient tile is added to the output with global atomics (halos of
 //      neighbouring tiles overlap).
 // No counterpart in the reference.
@@ -19,130 +20,132 @@
 
 namespace lpaici {
 
-// dst[m] += sum_{i + j = m} c[i] * w[j], m < len + P - 1; window slot m % P holds output m.
-template <int P>
-__device__ __forceinline__ void scatter_run(const float (&c)[P], float *dst, const float *__restrict__ w, int len) {
-    float acc[P];
+// dst[j] += sum_{i + k = j} c[i] * w_k for j < len + 3: the transpose of conv_run for one pixel row.
+// A window of 4 partial outputs slides along the run (slot j % 4 holds output j); every finished
+// output is added to shared memory with one atomic.  wq holds the run's duplicated weights.
+__device__ __forceinline__ void scatter_run(const float (&c)[4], float *dst, const float4 *__restrict__ wq, int len) {
+    float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    const int n_out = len + 3;
+    for (int j0 = 0; j0 < n_out; j0 += 4) {
 #pragma unroll
-    for (int i = 0; i < P; i++) acc[i] = 0.0f;
-    const int n_out = len + P - 1;
-    for (int j0 = 0; j0 < n_out; j0 += P) {
-#pragma unroll
-        for (int q = 0; q < P; q++) {
+        for (int q = 0; q < 4; q++) {
             const int j = j0 + q;
-            if (j < len) {
-                const float wt = w[j];
+            if (j < len) {  // taps of the run only (its weights are padded to an even count)
+                const float4 wp = wq[j >> 1];
+                const float w = (q & 1) ? wp.z : wp.x;
 #pragma unroll
-                for (int i = 0; i < P; i++) acc[(i + q) % P] = fmaf(c[i], wt, acc[(i + q) % P]);
+                for (int i = 0; i < 4; i++) acc[(i + q) & 3] = fmaf(c[i], w, acc[(i + q) & 3]);
             }
             if (j < n_out) {
-                atomicAdd(dst + j, acc[q]);  // output j is complete
+                atomicAdd(dst + j, acc[q]);
                 acc[q] = 0.0f;
             }
         }
     }
 }
 
-template <int P, int WX, int WY>
-__global__ void __launch_bounds__(32 * WX * WY)
+template <int WX, int WY>
+__global__ void __launch_bounds__(32 * WX * WY, 1)
     lpaici_backward_kernel(const __grid_constant__ ImageArgs img, const __grid_constant__ KernelTables tab) {
-    using Shape = TileShape<P, WX, WY>;
+    using Shape = TileShape<WX, WY>;
     extern __shared__ __align__(16) int smem[];
-    const int D = tab.D, S = tab.S, R = tab.R, nk = D * S;
-    const int tab_words = (2 * nk + 3) & ~3;
+    const int D = tab.D, S = tab.S, nk = D * S;
     int *s_blob = smem;
-    float *s_var = reinterpret_cast<float *>(smem + tab.blob_words);
-    float *s_thr = s_var + nk;
-    float *s_tile = reinterpret_cast<float *>(smem + tab.blob_words + tab_words);
-    const TileGeom g = TileGeom::make(Shape::kTileW, Shape::kTileH, R);
+    float *s_tab = reinterpret_cast<float *>(smem + tab.blob_words);
+    float2 *s_tile = reinterpret_cast<float2 *>(smem + tab.blob_words + table_words(nk));
+    float *s_grad = reinterpret_cast<float *>(s_tile);  // phase 2 reuses the tile's memory
+    const TileGeom g = TileGeom::make(Shape::kTileW, Shape::kTileH, tab.R);
+    const int R = g.R, gpitch = g.pitch2, grows = Shape::kTileH + 2 * R;
     const int x0 = blockIdx.x * Shape::kTileW, y0 = blockIdx.y * Shape::kTileH;
 
     stage_words(s_blob, tab.blob, tab.blob_words);
-    for (int i = threadIdx.x; i < nk; i += blockDim.x) {
-        s_var[i] = tab.var[i];
-        s_thr[i] = tab.thr[i];
-    }
-    load_tile(s_tile, img, x0, y0, R, g);
+    stage_tables(s_tab, tab.var, tab.thr, nk);
+    load_tile(s_tile, img, x0, y0, g);
     __syncthreads();
 
-    const LaneGeom<P, WX> lg;
+    const LaneGeom<WX> lg;
     const int oy = y0 + lg.ty, ox = x0 + lg.tx;
     unsigned valid = 0;
-    if (oy < img.rows_out) {
 #pragma unroll
-        for (int i = 0; i < P; i++)
-            if (ox + i < img.W) valid |= 1u << i;
-    }
-    const int lane_off = (lg.ty + R) * g.pitch + lg.tx + g.HL;
+    for (int i = 0; i < 8; i++)
+        if (oy + 8 * (i & 1) < img.rows_out && ox + (i >> 1) < img.W) valid |= 1u << i;
     const int4 *s_runs = reinterpret_cast<const int4 *>(s_blob + tab.run_word);
-    const float *s_w = reinterpret_cast<const float *>(s_blob + tab.weight_word);
+    const float4 *s_wq = reinterpret_cast<const float4 *>(s_blob + tab.weight_word);
+    const float *s_thr = s_tab + nk, *s_rvar = s_tab + 2 * nk;
 
-    // phase 1: selection of every direction, sum of the weights 1/v
-    unsigned long long sel[P];
-    float den[P];
+    // phase 1: the selection of every direction (4 bits each) and sum_d 1/v_d, per pixel
+    unsigned long long sel[8];
+    float den[8];
 #pragma unroll
-    for (int i = 0; i < P; i++) {
+    for (int i = 0; i < 8; i++) {
         sel[i] = 0ull;
         den[i] = 0.0f;
     }
+    const float2 *lane_tile = s_tile + (lg.ty + R) * g.pitch2 + lg.tx + R;
     for (int d = 0; d < D; d++) {
-        float best[P], bvar[P];
-        int sidx[P];
-        direction_sweep<P>(d, S, valid, s_tile + lane_off, g.pitch, s_blob, s_runs, s_w, s_var, s_thr, best, bvar,
-                           sidx);
+        float best[8];
+        unsigned sidx;
+        direction_sweep(d, S, valid, lane_tile, g.pitch2, s_blob, s_runs, s_wq, s_thr, best, sidx);
 #pragma unroll
-        for (int i = 0; i < P; i++) {
-            sel[i] |= static_cast<unsigned long long>(sidx[i]) << (4 * d);
-            den[i] = __fadd_rn(den[i], __fdiv_rn(1.0f, bvar[i]));
+        for (int i = 0; i < 8; i++) {
+            const unsigned si = (sidx >> (4 * i)) & 15u;
+            sel[i] |= static_cast<unsigned long long>(si) << (4 * d);
+            den[i] += s_rvar[d * S + si];
         }
     }
     __syncthreads();  // done reading the input tile
 
-    // phase 2: the tile becomes the gradient accumulator
-    for (int i = threadIdx.x; i < g.rows * g.pitch; i += blockDim.x) s_tile[i] = 0.0f;
-    float gp[P];
-    const float *gsrc = img.gout + static_cast<size_t>(oy) * img.gout_pitch + ox;
+    // phase 2: the tile's memory becomes the gradient accumulator (tile + R halo, plain floats)
+    for (int i = threadIdx.x; i < grows * gpitch; i += blockDim.x) s_grad[i] = 0.0f;
+    float gp[8];
 #pragma unroll
-    for (int i = 0; i < P; i++) gp[i] = (valid & (1u << i)) ? __ldg(gsrc + i) : 0.0f;
+    for (int i = 0; i < 8; i++)
+        gp[i] = (valid & (1u << i)) ? __ldg(img.gout + static_cast<size_t>(oy + 8 * (i & 1)) * img.gout_pitch + ox +
+                                            (i >> 1))
+                                    : 0.0f;
     __syncthreads();
 
-    float *lane_grad = s_tile + lane_off;
+    float *lane_grad = s_grad + (lg.ty + R) * gpitch + lg.tx + R;
     for (int d = 0; d < D; d++) {
-        float c[P];
+        float c[8];
         unsigned present = 0;
 #pragma unroll
-        for (int i = 0; i < P; i++) {
+        for (int i = 0; i < 8; i++) {
             const int s = static_cast<int>((sel[i] >> (4 * d)) & 15ull);
-            const float v = s_var[d * S + s];
-            c[i] = (valid & (1u << i)) ? gp[i] * ((1.0f / v) / den[i]) : 0.0f;
+            c[i] = (valid & (1u << i)) ? gp[i] * (s_rvar[d * S + s] / den[i]) : 0.0f;
             if (valid & (1u << i)) present |= 1u << s;
         }
         present = __reduce_or_sync(0xffffffffu, present);
         while (present) {
             const int s = __ffs(present) - 1;
             present &= present - 1;
-            float cs[P];
+            float c0[4], c1[4];  // rows ty and ty + 8
 #pragma unroll
-            for (int i = 0; i < P; i++) cs[i] = (static_cast<int>((sel[i] >> (4 * d)) & 15ull) == s) ? c[i] : 0.0f;
+            for (int m = 0; m < 4; m++) {
+                c0[m] = (static_cast<int>((sel[2 * m] >> (4 * d)) & 15ull) == s) ? c[2 * m] : 0.0f;
+                c1[m] = (static_cast<int>((sel[2 * m + 1] >> (4 * d)) & 15ull) == s) ? c[2 * m + 1] : 0.0f;
+            }
             const int k = d * S + s;
             const int rb = s_blob[k], re = s_blob[k + 1];
             for (int r = rb; r < re; r++) {
                 const int4 run = s_runs[r];
-                scatter_run<P>(cs, lane_grad + run.x * g.pitch + run.y, s_w + run.w, run.z);
+                float *dst = lane_grad + run.x * gpitch + run.y;
+                scatter_run(c0, dst, s_wq + (run.w >> 1), run.z);
+                scatter_run(c1, dst + 8 * gpitch, s_wq + (run.w >> 1), run.z);
             }
         }
     }
     __syncthreads();
 
     // phase 3: add the gradient tile (with its halo) to the output
-    const int gy0 = y0 + img.row_begin - R, gx0 = x0 - g.HL;
+    const int gy0 = y0 + img.row_begin - R, gx0 = x0 - R;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-    for (int r = warp; r < g.rows; r += nwarps) {
+    for (int r = warp; r < grows; r += nwarps) {
         const int gy = gy0 + r;
         if (gy < 0 || gy >= img.in_h) continue;
         float *dst = img.out + static_cast<size_t>(gy) * img.out_pitch;
-        const float *src = s_tile + r * g.pitch;
-        for (int cc = lane; cc < g.pitch; cc += 32) {
+        const float *src = s_grad + r * gpitch;
+        for (int cc = lane; cc < gpitch; cc += 32) {
             const int gx = gx0 + cc;
             if (gx >= 0 && gx < img.W) {
                 const float v = src[cc];
@@ -154,13 +157,15 @@ __global__ void __launch_bounds__(32 * WX * WY)
 
 namespace {
 
-template <int P, int WX, int WY>
+template <int WX, int WY>
 int launch_bwd(const ImageArgs &img, const KernelTables &tab, cudaStream_t stream) {
-    using Shape = TileShape<P, WX, WY>;
+    using Shape = TileShape<WX, WY>;
     const TileGeom g = TileGeom::make(Shape::kTileW, Shape::kTileH, tab.R);
     const int nk = tab.D * tab.S;
-    const size_t smem = sizeof(int) * (tab.blob_words + ((2 * nk + 3) & ~3)) + sizeof(float) * g.pitch * g.rows;
-    auto kern = lpaici_backward_kernel<P, WX, WY>;
+    const size_t grad_bytes = sizeof(float) * static_cast<size_t>(g.pitch2) * (Shape::kTileH + 2 * tab.R);
+    const size_t region = g.tile_bytes() > grad_bytes ? g.tile_bytes() : grad_bytes;
+    const size_t smem = sizeof(int) * (tab.blob_words + table_words(nk)) + region;
+    auto kern = lpaici_backward_kernel<WX, WY>;
     int dev = 0, max_optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
@@ -179,10 +184,18 @@ int launch_bwd(const ImageArgs &img, const KernelTables &tab, cudaStream_t strea
 
 }  // namespace
 
-int launch_backward(const lpaici_kernelset *ks, const ImageArgs &img, const KernelTables &tab, cudaStream_t stream) {
+#define LPAICI_BWD_CASE(idx, WX, WY) \
+    case idx: return launch_bwd<WX, WY>(img, tab, stream);
+
+int launch_backward(const lpaici_kernelset *ks, const ImageArgs &img, const KernelTables &tab, int config,
+                    cudaStream_t stream) {
     (void)ks;
-    return launch_bwd<9, 2, 4>(img, tab, stream);
+    switch (config) {
+        LPAICI_TILE_CONFIGS(LPAICI_BWD_CASE)
+        default: return set_error(LPAICI_ERR_INVALID_ARG, "tile config %d out of range", config);
+    }
 }
+#undef LPAICI_BWD_CASE
 
 }  // namespace lpaici
 
@@ -220,5 +233,5 @@ extern "C" int lpaici_backward(const lpaici_kernelset *ks, const float *d_noisy,
     KernelTables tab;
     fill_tables(ks, nullptr, sigma, gamma, &tab);
     tab.blob = blob;
-    return launch_backward(ks, img, tab, stream);
+    return launch_backward(ks, img, tab, default_config(ks), stream);
 }

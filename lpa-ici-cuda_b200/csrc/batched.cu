@@ -38,18 +38,16 @@ struct BatchArgs {
     int blob_words, run_word, weight_word;
 };
 
-template <int P, int WX, int WY>
-__global__ void __launch_bounds__(32 * WX * WY)
+template <int WX, int WY>
+__global__ void __launch_bounds__(32 * WX * WY, 1)
     lpaici_batched_kernel(const __grid_constant__ BatchArgs a) {
-    using Shape = TileShape<P, WX, WY>;
+    using Shape = TileShape<WX, WY>;
     extern __shared__ __align__(16) int smem[];
     __shared__ int s_item;
     const int nk = a.D * a.S;
-    const int tab_words = (2 * nk + 3) & ~3;
     int *s_blob = smem;
-    float *s_var = reinterpret_cast<float *>(smem + a.blob_words);
-    float *s_thr = s_var + nk;
-    float *s_tile = reinterpret_cast<float *>(smem + a.blob_words + tab_words);
+    float *s_tab = reinterpret_cast<float *>(smem + a.blob_words);
+    float2 *s_tile = reinterpret_cast<float2 *>(smem + a.blob_words + table_words(nk));
     const TileGeom g = TileGeom::make(Shape::kTileW, Shape::kTileH, a.R);
 
     stage_words(s_blob, a.blob, a.blob_words);
@@ -63,10 +61,7 @@ __global__ void __launch_bounds__(32 * WX * WY)
         const BatchImage bi = a.images[it.x];
         if (it.x != cur_image) {
             const float *t = a.tables + bi.tab_offset;
-            for (int i = threadIdx.x; i < nk; i += blockDim.x) {
-                s_var[i] = t[i];
-                s_thr[i] = t[nk + i];
-            }
+            stage_tables(s_tab, t, t + nk, nk);
             cur_image = it.x;
         }
         const int tiles_x = (bi.W + Shape::kTileW - 1) / Shape::kTileW;
@@ -82,9 +77,9 @@ __global__ void __launch_bounds__(32 * WX * WY)
         img.out_pitch = bi.out_pitch;
         img.row_begin = 0;
         img.rows_out = bi.H;
-        load_tile(s_tile, img, x0, y0, a.R, g);
+        load_tile(s_tile, img, x0, y0, g);
         __syncthreads();
-        sweep_tile<P, WX, WY>(img, x0, y0, a.D, a.S, a.R, g, s_blob, a.run_word, a.weight_word, s_var, s_thr, s_tile);
+        sweep_tile<WX>(img, x0, y0, a.D, a.S, g, s_blob, a.run_word, a.weight_word, s_tab, s_tile);
         __syncthreads();  // everyone done with s_tile / s_item before the next tile
     }
 }
@@ -97,22 +92,22 @@ struct KernelInfo {
     size_t smem;
 };
 
-template <int P, int WX, int WY>
+template <int WX, int WY>
 int batched_info(const KernelTables &tab, KernelInfo *info) {
-    using Shape = TileShape<P, WX, WY>;
+    using Shape = TileShape<WX, WY>;
     const TileGeom g = TileGeom::make(Shape::kTileW, Shape::kTileH, tab.R);
     const int nk = tab.D * tab.S;
-    info->fn = reinterpret_cast<const void *>(lpaici_batched_kernel<P, WX, WY>);
+    info->fn = reinterpret_cast<const void *>(lpaici_batched_kernel<WX, WY>);
     info->tile_w = Shape::kTileW;
     info->tile_h = Shape::kTileH;
     info->threads = Shape::kThreads;
-    info->smem = sizeof(int) * (tab.blob_words + ((2 * nk + 3) & ~3)) + sizeof(float) * g.pitch * g.rows;
+    info->smem = sizeof(int) * (tab.blob_words + table_words(nk)) + g.tile_bytes();
     return LPAICI_OK;
 }
 
 int get_info(int config, const KernelTables &tab, KernelInfo *info) {
-#define LPAICI_BATCH_CASE(idx, P, WX, WY) \
-    case idx: return batched_info<P, WX, WY>(tab, info);
+#define LPAICI_BATCH_CASE(idx, WX, WY) \
+    case idx: return batched_info<WX, WY>(tab, info);
     switch (config) {
         LPAICI_TILE_CONFIGS(LPAICI_BATCH_CASE)
         default: return set_error(LPAICI_ERR_INVALID_ARG, "tile config %d out of range", config);

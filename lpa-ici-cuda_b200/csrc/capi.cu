@@ -12,13 +12,17 @@ using namespace lpaici;
 namespace lpaici {
 
 int default_config(const lpaici_kernelset *ks) {
-    int dev = 0;
+    int dev = 0, max_optin = 0;
     if (cudaGetDevice(&dev) == cudaSuccess) {
         std::lock_guard<std::mutex> lock(ks->mu);
         if (dev < static_cast<int>(ks->tuned_config.size()) && ks->tuned_config[dev] >= 0)
             return ks->tuned_config[dev];
     }
-    return LPAICI_DEFAULT_TILE_CONFIG;
+    cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    for (int c = 0; c < LPAICI_NUM_TILE_CONFIGS; c++)
+        if (config_smem(c, ks->layout.total_words, ks->D * ks->S, ks->radius) <= static_cast<size_t>(max_optin))
+            return c;
+    return LPAICI_DEFAULT_TILE_CONFIG;  // nothing fits: the launch reports LPAICI_ERR_UNSUPPORTED
 }
 
 static int check_params(float sigma_or_one, float gamma) {
@@ -97,12 +101,12 @@ int lpaici_forward_rows(const lpaici_kernelset *ks, const float *d_in, int in_pi
 int lpaici_num_tile_configs(void) { return LPAICI_NUM_TILE_CONFIGS; }
 
 int lpaici_tile_config_desc(int index, int *tile_w, int *tile_h, int *threads, int *pixels_per_thread) {
-#define LPAICI_DESC_CASE(idx, P, WX, WY)                  \
-    case idx:                                             \
-        if (tile_w) *tile_w = (WX) * 4 * (P);             \
-        if (tile_h) *tile_h = (WY) * 8;                   \
-        if (threads) *threads = 32 * (WX) * (WY);         \
-        if (pixels_per_thread) *pixels_per_thread = (P);  \
+#define LPAICI_DESC_CASE(idx, WX, WY)                    \
+    case idx:                                            \
+        if (tile_w) *tile_w = (WX) * 16;                 \
+        if (tile_h) *tile_h = (WY) * 16;                 \
+        if (threads) *threads = 32 * (WX) * (WY);        \
+        if (pixels_per_thread) *pixels_per_thread = 8;   \
         return LPAICI_OK;
     switch (index) {
         LPAICI_TILE_CONFIGS(LPAICI_DESC_CASE)

@@ -11,40 +11,34 @@
 
 namespace lpaici {
 
-template <int P, int WX, int WY>
-__global__ void __launch_bounds__(32 * WX * WY)
+template <int WX, int WY>
+__global__ void __launch_bounds__(32 * WX * WY, 1)
     lpaici_forward_kernel(const __grid_constant__ ImageArgs img, const __grid_constant__ KernelTables tab) {
-    using Shape = TileShape<P, WX, WY>;
+    using Shape = TileShape<WX, WY>;
     extern __shared__ __align__(16) int smem[];
     const int nk = tab.D * tab.S;
-    const int tab_words = (2 * nk + 3) & ~3;
     int *s_blob = smem;
-    float *s_var = reinterpret_cast<float *>(smem + tab.blob_words);
-    float *s_thr = s_var + nk;
-    float *s_tile = reinterpret_cast<float *>(smem + tab.blob_words + tab_words);
+    float *s_tab = reinterpret_cast<float *>(smem + tab.blob_words);
+    float2 *s_tile = reinterpret_cast<float2 *>(smem + tab.blob_words + table_words(nk));
     const TileGeom g = TileGeom::make(Shape::kTileW, Shape::kTileH, tab.R);
     const int x0 = blockIdx.x * Shape::kTileW, y0 = blockIdx.y * Shape::kTileH;
 
     stage_words(s_blob, tab.blob, tab.blob_words);
-    for (int i = threadIdx.x; i < nk; i += blockDim.x) {
-        s_var[i] = tab.var[i];
-        s_thr[i] = tab.thr[i];
-    }
-    load_tile(s_tile, img, x0, y0, tab.R, g);
+    stage_tables(s_tab, tab.var, tab.thr, nk);
+    load_tile(s_tile, img, x0, y0, g);
     __syncthreads();
-    sweep_tile<P, WX, WY>(img, x0, y0, tab.D, tab.S, tab.R, g, s_blob, tab.run_word, tab.weight_word, s_var, s_thr,
-                          s_tile);
+    sweep_tile<WX>(img, x0, y0, tab.D, tab.S, g, s_blob, tab.run_word, tab.weight_word, s_tab, s_tile);
 }
 
 namespace {
 
-template <int P, int WX, int WY>
+template <int WX, int WY>
 int launch_cfg(const ImageArgs &img, const KernelTables &tab, cudaStream_t stream) {
-    using Shape = TileShape<P, WX, WY>;
+    using Shape = TileShape<WX, WY>;
     const TileGeom g = TileGeom::make(Shape::kTileW, Shape::kTileH, tab.R);
     const int nk = tab.D * tab.S;
-    const size_t smem = sizeof(int) * (tab.blob_words + ((2 * nk + 3) & ~3)) + sizeof(float) * g.pitch * g.rows;
-    auto kern = lpaici_forward_kernel<P, WX, WY>;
+    const size_t smem = sizeof(int) * (tab.blob_words + table_words(nk)) + g.tile_bytes();
+    auto kern = lpaici_forward_kernel<WX, WY>;
     int dev = 0, max_optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
@@ -63,8 +57,24 @@ int launch_cfg(const ImageArgs &img, const KernelTables &tab, cudaStream_t strea
 
 }  // namespace
 
-#define LPAICI_FWD_CASE(idx, P, WX, WY) \
-    case idx: return launch_cfg<P, WX, WY>(img, tab, stream);
+#define LPAICI_FWD_CASE(idx, WX, WY) \
+    case idx: return launch_cfg<WX, WY>(img, tab, stream);
+
+// Shared memory a tile configuration needs for a kernel set: blob + tables + the larger of the
+// T8 tile (forward) and the plain gradient tile (adjoint).
+size_t config_smem(int config, int blob_words, int nk, int R) {
+#define LPAICI_SMEM_CASE(idx, WX, WY)                                                                  \
+    case idx: {                                                                                        \
+        const TileGeom g = TileGeom::make(16 * (WX), 16 * (WY), R);                                   \
+        const size_t grad = sizeof(float) * static_cast<size_t>(g.pitch2) * (16 * (WY) + 2 * R);       \
+        return sizeof(int) * (blob_words + table_words(nk)) + (g.tile_bytes() > grad ? g.tile_bytes() : grad); \
+    }
+    switch (config) {
+        LPAICI_TILE_CONFIGS(LPAICI_SMEM_CASE)
+        default: return ~size_t(0);
+    }
+#undef LPAICI_SMEM_CASE
+}
 
 int launch_forward(const lpaici_kernelset *ks, const ImageArgs &img, const KernelTables &tab, int config,
                    cudaStream_t stream) {

@@ -17,18 +17,19 @@ namespace lpaici {
 constexpr int kMaxKernels = 256;
 constexpr int kMaxRadius = 127;
 
-// One row run of a kernel, as the device reads it: the taps (dy, dx0 + j), j < len, with weights
-// weights[woff + j].  dy/dx0 are offsets from the output pixel (row - rows/2, col - cols/2).
+// One row run of a kernel, as the device reads it: the taps (dy, dx0 + j), j < len, whose weights
+// are wdup[wofs + j] = {w_j, w_j}.  dy/dx0 are offsets from the output pixel
+// (row - rows/2, col - cols/2); wofs is even, so two taps' duplicated weights are one 16-byte load.
 struct Run {
-    int dy, dx0, len, woff;
+    int dy, dx0, len, wofs;
 };
 
 // Device image of a kernel set, one contiguous block of 32-bit words:
-//   [0, nk+1)                 first run of kernel k (kernel k's runs are [begin[k], begin[k+1]))
-//   [run_word, +4*n_runs)     Run records, 16-byte aligned
-//   [weight_word, +n_taps)    packed weights
+//   [0, nk+1)               first run of kernel k (kernel k's runs are [begin[k], begin[k+1]))
+//   [run_word, +4*n_runs)   Run records, 16-byte aligned
+//   [weight_word, ...)      float2 {w, w} per tap, every run padded to an even number of taps
 struct BlobLayout {
-    int nk = 0, n_runs = 0, n_taps = 0;
+    int nk = 0, n_runs = 0, n_wdup = 0;
     int run_word = 0, weight_word = 0, total_words = 0;  // total padded to a multiple of 4
 };
 
@@ -90,7 +91,11 @@ void fill_tables(const lpaici_kernelset *ks, const float *var_or_null, float sig
 // Forward / backward launchers (forward.cu, backward.cu).
 int launch_forward(const lpaici_kernelset *ks, const ImageArgs &img, const KernelTables &tab, int config,
                    cudaStream_t stream);
-int launch_backward(const lpaici_kernelset *ks, const ImageArgs &img, const KernelTables &tab, cudaStream_t stream);
+int launch_backward(const lpaici_kernelset *ks, const ImageArgs &img, const KernelTables &tab, int config,
+                    cudaStream_t stream);
+// Bytes of shared memory tile configuration `config` needs for a kernel set (forward and adjoint).
+size_t config_smem(int config, int blob_words, int nk, int R);
+// The autotuned configuration of ks on the current device, else the first one that fits.
 int default_config(const lpaici_kernelset *ks);
 
 }  // namespace lpaici

@@ -78,32 +78,38 @@ static int finish_kernelset(lpaici_kernelset *ks) {
     if (ks->radius > kMaxRadius)
         return set_error(LPAICI_ERR_UNSUPPORTED, "kernel radius %d exceeds the supported %d", ks->radius, kMaxRadius);
 
-    // device blob: [run begin per kernel (nk+1)] [Run records] [weights]
+    // device blob: [run begin per kernel (nk+1)] [Run records] [{w, w} per tap, runs padded to even]
     BlobLayout &L = ks->layout;
     L.nk = nk;
     L.n_runs = static_cast<int>(ks->run_row.size());
-    L.n_taps = static_cast<int>(ks->run_w.size());
     L.run_word = (nk + 1 + 3) & ~3;
     L.weight_word = L.run_word + 4 * L.n_runs;
-    L.total_words = (L.weight_word + L.n_taps + 3) & ~3;
+    std::vector<int> wofs(L.n_runs);
+    int n2 = 0;
+    for (int r = 0; r < L.n_runs; r++) {
+        wofs[r] = n2;
+        n2 += (ks->run_len[r] + 1) & ~1;
+    }
+    L.n_wdup = n2;
+    L.total_words = (L.weight_word + 2 * n2 + 3) & ~3;
     ks->blob.assign(L.total_words, 0);
     for (int k = 0; k < nk; k++) ks->blob[k] = ks->k_first_run[k];
     ks->blob[nk] = L.n_runs;
-    for (int r = 0; r < L.n_runs; r++) {
-        ks->blob[L.run_word + 4 * r + 0] = ks->run_row[r];
-        ks->blob[L.run_word + 4 * r + 1] = ks->run_col[r];
-        ks->blob[L.run_word + 4 * r + 2] = ks->run_len[r];
-        ks->blob[L.run_word + 4 * r + 3] = 0;
-    }
-    // woff: index of the run's first weight; runs are packed back to back per kernel
+    float *wd = reinterpret_cast<float *>(ks->blob.data() + L.weight_word);
     for (int k = 0; k < nk; k++) {
         int w = ks->k_first_weight[k];
         for (int r = ks->k_first_run[k]; r < ks->k_first_run[k] + ks->k_num_runs[k]; r++) {
-            ks->blob[L.run_word + 4 * r + 3] = w;
+            ks->blob[L.run_word + 4 * r + 0] = ks->run_row[r];
+            ks->blob[L.run_word + 4 * r + 1] = ks->run_col[r];
+            ks->blob[L.run_word + 4 * r + 2] = ks->run_len[r];
+            ks->blob[L.run_word + 4 * r + 3] = wofs[r];
+            for (int j = 0; j < ks->run_len[r]; j++) {
+                wd[2 * (wofs[r] + j)] = ks->run_w[w + j];
+                wd[2 * (wofs[r] + j) + 1] = ks->run_w[w + j];
+            }
             w += ks->run_len[r];
         }
     }
-    std::memcpy(ks->blob.data() + L.weight_word, ks->run_w.data(), sizeof(float) * L.n_taps);
     return LPAICI_OK;
 }
 

@@ -1,84 +1,100 @@
-// tile_core.cuh -- the per-tile LPA-ICI forward sweep shared by the single-image and the batched
-// (persistent) kernels.
+// tile_core.cuh -- the per-tile LPA-ICI sweep shared by the single-image, batched and adjoint kernels.
 //
-// Layout of one CTA's shared memory:
-//   blob   the packed kernel set (BlobLayout): run ranges, Run records, weights
-//   tab    var[nk], thr[nk] of the image being processed
-//   tile   (TH + 2R) rows x pitch floats: the input window of the output tile plus a halo of R rows
-//          above/below, HL = align4(R) columns left and >= R right; zero outside the image
+// Shared memory of one CTA:
+//   blob   the packed kernel set (BlobLayout): run ranges, Run records, duplicated weights {w, w}
+//   tab    var[nk], thr[nk], rvar[nk] = 1/var of the image being processed
+//   tile   T8[j][c] = {x(j, c), x(j + 8, c)}: the input window of the output tile as pairs of rows
+//          8 apart, j < TH - 8 + 2R, c < pitch2 (odd); input row j is output row j - R of the tile,
+//          input column c is output column c - R; zero outside the input
 //
-// Thread mapping: a warp covers 8 rows x (4 lanes x P) columns; lane = 4*row + quarter.  Each
-// thread owns P horizontally adjacent pixels.  With P odd and pitch/4 odd the 32 lanes of a scalar
-// shared-memory load hit 32 different banks (rows give the 8 multiples of 4, the lane's column
-// offset quarter*P gives the 4 residues mod 4).
+// Thread mapping: a warp covers 16 rows x 16 columns; lane = 4a + b owns the 8 pixels of rows
+// (a, a + 8) and columns 4b .. 4b + 3 of its warp's block, held as 4 float2 pairs {row a, row a+8}.
+// Every window value is then a natural register pair, so one packed __fmul2_rn / __fadd2_rn does two
+// pixels' taps.  A 16-lane half-warp's 8-byte loads hit 16 different bank pairs (pitch2 odd: the 4
+// rows give 4 residues mod 4, the column groups 4b the multiples of 4).
 //
 // Arithmetic (bit-identical to src/v1_0_lpa_ici_2D_fused.cpp:803-930 for finite inputs):
-//   conv  = sum over the kernel's taps in row-major order of __fmul_rn(w, x), added with __fadd_rn,
-//           starting from +0.0f; zero-filled halo taps add +-0, which changes nothing (a running sum
+//   conv  = sum over the kernel's taps in row-major order of w*x (rounded), added one by one with
+//           round-to-nearest, starting from +0.0f -- packed f32x2 instructions round each half on its
+//           own; zero-filled halo taps and zero weights add +-0, which changes nothing (a running sum
 //           started at +0 never becomes -0);
 //   lb/ub = conv -+ thr;  lo = max(lo, lb); hi = min(hi, ub); accept while hi >= lo, else stop;
-//   num  += est * (1/var); den += 1/var (in direction order);  out = num / den.
+//   num  += est * (1/var); den += 1/var (in direction order, 1/var correctly rounded);  out = num / den.
 #pragma once
 
 #include "internal.h"
 
 namespace lpaici {
 
-// Smallest pitch >= need with pitch % 4 == 0 and (pitch / 4) odd (conflict-free rows, 16 B rows).
-__host__ __device__ inline int tile_pitch(int need) {
-    int p = (need + 3) & ~3;
-    if (((p >> 2) & 1) == 0) p += 4;
-    return p;
-}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 
-template <int P, int WX, int WY>
+// Smallest odd pitch (in float2) >= need.
+__host__ __device__ inline int tile_pitch2(int need) { return need | 1; }
+
+template <int WX, int WY>
 struct TileShape {
-    static constexpr int kPixels = P;
     static constexpr int kThreads = 32 * WX * WY;
-    static constexpr int kTileW = WX * 4 * P;
-    static constexpr int kTileH = WY * 8;
+    static constexpr int kTileW = WX * 16;
+    static constexpr int kTileH = WY * 16;
 };
 
-// Smem geometry of a tile for radius R.
+// Shared-memory geometry of a tile for radius R.
 struct TileGeom {
-    int HL, pitch, rows;
+    int R, pitch2, pairs;  // pairs: number of T8 rows
     __host__ __device__ static TileGeom make(int tile_w, int tile_h, int R) {
         TileGeom g;
-        g.HL = (R + 3) & ~3;
-        g.pitch = tile_pitch(g.HL + tile_w + R);
-        g.rows = tile_h + 2 * R;
+        g.R = R;
+        g.pitch2 = tile_pitch2(tile_w + 2 * R);
+        g.pairs = tile_h - 8 + 2 * R;
         return g;
     }
+    __host__ __device__ size_t tile_bytes() const { return sizeof(float2) * static_cast<size_t>(pitch2) * pairs; }
 };
 
-// acc[i] += sum_{j < len} w[j] * src[i + j], for the P pixels of a thread, tap by tap in order.
-// The window holds src[m] in slot m % P; every step loads one new value.
-template <int P>
-__device__ __forceinline__ void conv_run(float (&acc)[P], const float *__restrict__ src, const float *__restrict__ w,
-                                         int len) {
-    float win[P];
-#pragma unroll
-    for (int i = 0; i < P - 1; i++) win[i] = src[i];
-    int k = 0;
-    for (; k + P <= len; k += P) {
-#pragma unroll
-        for (int j = 0; j < P; j++) {
-            win[(j + P - 1) % P] = src[k + j + P - 1];
-            const float wt = w[k + j];
-#pragma unroll
-            for (int i = 0; i < P; i++) acc[i] = __fadd_rn(acc[i], __fmul_rn(wt, win[(j + i) % P]));
-        }
+// Words of shared memory before the tile: the blob, then var/thr/rvar (padded to 16 bytes).
+__host__ __device__ inline int table_words(int nk) { return (3 * nk + 3) & ~3; }
+
+// One tap column of the sliding window: win slot (j + 3) % 4 receives column k + j + 3, then the
+// 4 pixel pairs m accumulate w * column (k + j + m).
+#define LPAICI_STEP(J, WX_, WY_)                                              \
+    {                                                                         \
+        win[((J) + 3) & 3] = src[k + (J) + 3];                                \
+        const float2 w2 = make_float2(WX_, WY_);                              \
+        _Pragma("unroll") for (int m = 0; m < 4; m++) acc[m] = add2(acc[m], mul2(w2, win[((J) + m) & 3])); \
     }
-#pragma unroll
-    for (int j = 0; j < P - 1; j++) {
-        if (k + j < len) {
-            win[(j + P - 1) % P] = src[k + j + P - 1];
-            const float wt = w[k + j];
-#pragma unroll
-            for (int i = 0; i < P; i++) acc[i] = __fadd_rn(acc[i], __fmul_rn(wt, win[(j + i) % P]));
+
+// acc[m] += sum_{j < len} {w_j, w_j} * src[m + j], tap by tap in order, for the 4 pixel pairs.
+// src: the run's first column in T8 (row already chosen); wq: the run's duplicated weights as
+// float4 {w_2i, w_2i, w_2i+1, w_2i+1}.
+__device__ __forceinline__ void conv_run(float2 (&acc)[4], const float2 *__restrict__ src,
+                                         const float4 *__restrict__ wq, int len) {
+    float2 win[4];
+    win[0] = src[0];
+    win[1] = src[1];
+    win[2] = src[2];
+    int k = 0;
+    for (; k + 4 <= len; k += 4) {
+        const float4 wa = wq[k >> 1], wb = wq[(k >> 1) + 1];
+        LPAICI_STEP(0, wa.x, wa.y)
+        LPAICI_STEP(1, wa.z, wa.w)
+        LPAICI_STEP(2, wb.x, wb.y)
+        LPAICI_STEP(3, wb.z, wb.w)
+    }
+    const int rem = len - k;  // 0..3, warp-uniform
+    if (rem > 0) {
+        const float4 wa = wq[k >> 1];
+        LPAICI_STEP(0, wa.x, wa.y)
+        if (rem > 1) {
+            LPAICI_STEP(1, wa.z, wa.w)
+            if (rem > 2) {
+                const float4 wb = wq[(k >> 1) + 1];  // the second tap of this float4 is padding
+                LPAICI_STEP(2, wb.x, wb.y)
+            }
         }
     }
 }
+#undef LPAICI_STEP
 
 // Copies `words` 32-bit words (a multiple of 4, 16-byte aligned) from global to shared memory.
 __device__ __forceinline__ void stage_words(int *dst, const int *__restrict__ src, int words) {
@@ -87,76 +103,89 @@ __device__ __forceinline__ void stage_words(int *dst, const int *__restrict__ sr
     for (int i = threadIdx.x; i < (words >> 2); i += blockDim.x) d[i] = __ldg(s + i);
 }
 
-// Loads the halo'd input window of the output tile whose top-left output pixel is (x0, y0).
-// Input pixel (gy, gx) with gy = y0 + row_begin - R + r, gx = x0 - HL + c; zero outside the input.
-__device__ __forceinline__ void load_tile(float *s_tile, const ImageArgs &img, int x0, int y0, int R,
-                                          const TileGeom &g) {
+// var, thr and rvar = 1/var (correctly rounded, the reference's 1.0f / var_d) into shared memory.
+__device__ __forceinline__ void stage_tables(float *s_tab, const float *var, const float *thr, int nk) {
+    for (int i = threadIdx.x; i < nk; i += blockDim.x) {
+        s_tab[i] = var[i];
+        s_tab[nk + i] = thr[i];
+        s_tab[2 * nk + i] = __fdiv_rn(1.0f, var[i]);
+    }
+}
+
+// Builds T8 for the output tile whose top-left output pixel is (x0, y0): input pixel
+// (gy0 + j, gx0 + c) and (gy0 + j + 8, gx0 + c), gy0 = y0 + row_begin - R, gx0 = x0 - R.
+__device__ __forceinline__ void load_tile(float2 *s_tile, const ImageArgs &img, int x0, int y0, const TileGeom &g) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-    const int gy0 = y0 + img.row_begin - R, gx0 = x0 - g.HL;
-    for (int r = warp; r < g.rows; r += nwarps) {
-        const int gy = gy0 + r;
-        const bool row_ok = gy >= 0 && gy < img.in_h;
-        const float *src = img.in + static_cast<size_t>(row_ok ? gy : 0) * img.in_pitch;
-        float *dst = s_tile + r * g.pitch;
-        for (int c = lane; c < g.pitch; c += 32) {
+    const int gy0 = y0 + img.row_begin - g.R, gx0 = x0 - g.R;
+    for (int j = warp; j < g.pairs; j += nwarps) {
+        const int ga = gy0 + j, gb = ga + 8;
+        const bool ok_a = ga >= 0 && ga < img.in_h, ok_b = gb >= 0 && gb < img.in_h;
+        const float *ra = img.in + static_cast<size_t>(ok_a ? ga : 0) * img.in_pitch;
+        const float *rb = img.in + static_cast<size_t>(ok_b ? gb : 0) * img.in_pitch;
+        float2 *dst = s_tile + j * g.pitch2;
+        for (int c = lane; c < g.pitch2; c += 32) {
             const int gx = gx0 + c;
-            dst[c] = (row_ok && gx >= 0 && gx < img.W) ? __ldg(src + gx) : 0.0f;
+            const bool ok_x = gx >= 0 && gx < img.W;
+            dst[c] = make_float2(ok_a && ok_x ? __ldg(ra + gx) : 0.0f, ok_b && ok_x ? __ldg(rb + gx) : 0.0f);
         }
     }
 }
 
-// Lane geometry of a thread inside its tile.
-template <int P, int WX>
+// Lane geometry inside the tile: rows ty and ty + 8, columns tx .. tx + 3 (tile-local output).
+template <int WX>
 struct LaneGeom {
-    int ty, tx;  // tile-local row and first column of the thread's P pixels
+    int ty, tx;
     __device__ __forceinline__ LaneGeom() {
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        ty = (warp / WX) * 8 + (lane >> 2);
-        tx = (warp % WX) * 4 * P + (lane & 3) * P;
+        ty = (warp / WX) * 16 + (lane >> 2);
+        tx = (warp % WX) * 16 + (lane & 3) * 4;
     }
 };
 
-// The ICI scale sweep of one direction d for the thread's P pixels (mask `valid`): for every
-// pixel the estimate, variance and index of the last accepted scale.  Warp-uniform loop over the
-// scales; it ends when every pixel of the warp has stopped.
-template <int P>
-__device__ __forceinline__ void direction_sweep(int d, int S, unsigned valid, const float *lane_tile, int pitch,
-                                                const int *s_blob, const int4 *s_runs, const float *s_w,
-                                                const float *s_var, const float *s_thr, float (&best)[P],
-                                                float (&bvar)[P], int (&sidx)[P]) {
-    float lo[P], hi[P];
+// Pixel i = 2m + h of a thread: column tx + m, row ty + 8h.
+__device__ __forceinline__ float pick(const float2 (&v)[4], int i) { return (i & 1) ? v[i >> 1].y : v[i >> 1].x; }
+
+// The ICI scale sweep of direction d for the thread's 8 pixels (mask `valid`): estimate and index
+// of the last accepted scale of every pixel (sidx: 4 bits per pixel).  Warp-uniform scale loop; it
+// ends when every pixel of the warp has stopped.
+__device__ __forceinline__ void direction_sweep(int d, int S, unsigned valid, const float2 *lane_tile, int pitch2,
+                                                const int *s_blob, const int4 *s_runs, const float4 *s_wq,
+                                                const float *s_thr, float (&best)[8], unsigned &sidx) {
+    float lo[8], hi[8];
 #pragma unroll
-    for (int i = 0; i < P; i++) {
+    for (int i = 0; i < 8; i++) {
         lo[i] = -INFINITY;
         hi[i] = INFINITY;
         best[i] = 0.0f;
-        bvar[i] = 0.0f;
-        sidx[i] = 0;
     }
+    sidx = 0;
     unsigned alive = valid;
     for (int s = 0; s < S; s++) {
         if (!__any_sync(0xffffffffu, alive)) break;  // every pixel of the warp has stopped
         const int k = d * S + s;
-        float acc[P];
+        float2 acc[4];
 #pragma unroll
-        for (int i = 0; i < P; i++) acc[i] = 0.0f;
+        for (int m = 0; m < 4; m++) acc[m] = make_float2(0.0f, 0.0f);
         const int rb = s_blob[k], re = s_blob[k + 1];
         for (int r = rb; r < re; r++) {
             const int4 run = s_runs[r];
-            conv_run<P>(acc, lane_tile + run.x * pitch + run.y, s_w + run.w, run.z);
+            conv_run(acc, lane_tile + run.x * pitch2 + run.y, s_wq + (run.w >> 1), run.z);
         }
-        const float thr = s_thr[k], var = s_var[k];
+        const float thr = s_thr[k];
+        float2 lb[4], ub[4];
 #pragma unroll
-        for (int i = 0; i < P; i++) {
+        for (int m = 0; m < 4; m++) {
+            lb[m] = add2(acc[m], make_float2(-thr, -thr));  // conv - thr, exactly
+            ub[m] = add2(acc[m], make_float2(thr, thr));
+        }
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
             if (alive & (1u << i)) {
-                const float lb = __fsub_rn(acc[i], thr);
-                const float ub = __fadd_rn(acc[i], thr);
-                lo[i] = fmaxf(lo[i], lb);
-                hi[i] = fminf(hi[i], ub);
+                lo[i] = fmaxf(lo[i], pick(lb, i));
+                hi[i] = fminf(hi[i], pick(ub, i));
                 if (hi[i] >= lo[i]) {
-                    best[i] = acc[i];
-                    bvar[i] = var;
-                    sidx[i] = s;
+                    best[i] = pick(acc, i);
+                    sidx = (sidx & ~(15u << (4 * i))) | (static_cast<unsigned>(s) << (4 * i));
                 } else {
                     alive &= ~(1u << i);
                 }
@@ -165,48 +194,51 @@ __device__ __forceinline__ void direction_sweep(int d, int S, unsigned valid, co
     }
 }
 
-// The forward sweep of one tile (tile already in shared memory, block-synchronised).
-template <int P, int WX, int WY>
-__device__ __forceinline__ void sweep_tile(const ImageArgs &img, int x0, int y0, int D, int S, int R,
-                                           const TileGeom &g, const int *s_blob, int run_word, int weight_word,
-                                           const float *s_var, const float *s_thr, const float *s_tile) {
-    const LaneGeom<P, WX> lg;
+// The forward sweep of one tile (tile in shared memory, block-synchronised).
+template <int WX>
+__device__ __forceinline__ void sweep_tile(const ImageArgs &img, int x0, int y0, int D, int S, const TileGeom &g,
+                                           const int *s_blob, int run_word, int weight_word, const float *s_tab,
+                                           const float2 *s_tile) {
+    const LaneGeom<WX> lg;
+    const int nk = D * S;
     const int oy = y0 + lg.ty, ox = x0 + lg.tx;
     unsigned valid = 0;
-    if (oy < img.rows_out) {
 #pragma unroll
-        for (int i = 0; i < P; i++)
-            if (ox + i < img.W) valid |= 1u << i;
-    }
-    const float *lane_tile = s_tile + (lg.ty + R) * g.pitch + lg.tx + g.HL;
+    for (int i = 0; i < 8; i++)
+        if (oy + 8 * (i & 1) < img.rows_out && ox + (i >> 1) < img.W) valid |= 1u << i;
+    const float2 *lane_tile = s_tile + (lg.ty + g.R) * g.pitch2 + lg.tx + g.R;
     const int4 *s_runs = reinterpret_cast<const int4 *>(s_blob + run_word);
-    const float *s_w = reinterpret_cast<const float *>(s_blob + weight_word);
+    const float4 *s_wq = reinterpret_cast<const float4 *>(s_blob + weight_word);
+    const float *s_thr = s_tab + nk, *s_rvar = s_tab + 2 * nk;
 
-    float num[P], den[P];
+    float2 num[4], den[4];
 #pragma unroll
-    for (int i = 0; i < P; i++) num[i] = den[i] = 0.0f;
+    for (int m = 0; m < 4; m++) num[m] = den[m] = make_float2(0.0f, 0.0f);
 
     for (int d = 0; d < D; d++) {
-        float best[P], bvar[P];
-        int sidx[P];
-        direction_sweep<P>(d, S, valid, lane_tile, g.pitch, s_blob, s_runs, s_w, s_var, s_thr, best, bvar, sidx);
+        float best[8];
+        unsigned sidx;
+        direction_sweep(d, S, valid, lane_tile, g.pitch2, s_blob, s_runs, s_wq, s_thr, best, sidx);
 #pragma unroll
-        for (int i = 0; i < P; i++) {
-            const float rcp = __fdiv_rn(1.0f, bvar[i]);
-            num[i] = __fadd_rn(num[i], __fmul_rn(best[i], rcp));
-            den[i] = __fadd_rn(den[i], rcp);
+        for (int m = 0; m < 4; m++) {
+            const float2 r = make_float2(s_rvar[d * S + ((sidx >> (8 * m)) & 15)],
+                                         s_rvar[d * S + ((sidx >> (8 * m + 4)) & 15)]);
+            num[m] = add2(num[m], mul2(make_float2(best[2 * m], best[2 * m + 1]), r));
+            den[m] = add2(den[m], r);
         }
         if (img.smap) {
-            uint8_t *m = img.smap + (static_cast<size_t>(d) * img.rows_out + oy) * img.W + ox;
 #pragma unroll
-            for (int i = 0; i < P; i++)
-                if (valid & (1u << i)) m[i] = static_cast<uint8_t>(sidx[i]);
+            for (int i = 0; i < 8; i++)
+                if (valid & (1u << i))
+                    img.smap[(static_cast<size_t>(d) * img.rows_out + oy + 8 * (i & 1)) * img.W + ox + (i >> 1)] =
+                        static_cast<uint8_t>((sidx >> (4 * i)) & 15);
         }
     }
-    float *o = img.out + static_cast<size_t>(oy) * img.out_pitch + ox;
 #pragma unroll
-    for (int i = 0; i < P; i++)
-        if (valid & (1u << i)) o[i] = __fdiv_rn(num[i], den[i]);
+    for (int i = 0; i < 8; i++)
+        if (valid & (1u << i))
+            img.out[static_cast<size_t>(oy + 8 * (i & 1)) * img.out_pitch + ox + (i >> 1)] =
+                __fdiv_rn(pick(num, i), pick(den, i));
 }
 
 }  // namespace lpaici
