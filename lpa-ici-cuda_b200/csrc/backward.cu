@@ -85,7 +85,8 @@ __global__ void __launch_bounds__(32 * WX * WY, 1)
     for (int d = 0; d < D; d++) {
         float best[8];
         unsigned sidx;
-        direction_sweep(d, S, valid, lane_tile, g.pitch2, s_blob, s_runs, s_wq, s_thr, best, sidx);
+        direction_sweep(d, S, valid, lane_tile, g.pitch2, s_blob, s_runs, s_wq, s_thr,
+                        make_float2(tab.neg_zero, tab.neg_zero), best, sidx);
 #pragma unroll
         for (int i = 0; i < 8; i++) {
             const unsigned si = (sidx >> (4 * i)) & 15u;

@@ -36,6 +36,7 @@ struct BatchArgs {
     int D, S, R;
     const int *blob;
     int blob_words, run_word, weight_word;
+    float neg_zero;  // -0.0f, read at run time (see prod2 in tile_core.cuh)
 };
 
 template <int WX, int WY>
@@ -79,7 +80,7 @@ __global__ void __launch_bounds__(32 * WX * WY, 1)
         img.rows_out = bi.H;
         load_tile(s_tile, img, x0, y0, g);
         __syncthreads();
-        sweep_tile<WX>(img, x0, y0, a.D, a.S, g, s_blob, a.run_word, a.weight_word, s_tab, s_tile);
+        sweep_tile<WX>(img, x0, y0, a.D, a.S, g, s_blob, a.run_word, a.weight_word, s_tab, s_tile, a.neg_zero);
         __syncthreads();  // everyone done with s_tile / s_item before the next tile
     }
 }
@@ -247,6 +248,7 @@ int lpaici_batch_create(const lpaici_kernelset *ks, const lpaici_image *images, 
     b->args.blob_words = tab.blob_words;
     b->args.run_word = tab.run_word;
     b->args.weight_word = tab.weight_word;
+    b->args.neg_zero = -0.0f;
 
     int max_optin = 0, sms = 0, per_sm = 0;
     cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device);

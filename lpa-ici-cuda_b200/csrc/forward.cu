@@ -27,7 +27,8 @@ __global__ void __launch_bounds__(32 * WX * WY, 1)
     stage_tables(s_tab, tab.var, tab.thr, nk);
     load_tile(s_tile, img, x0, y0, g);
     __syncthreads();
-    sweep_tile<WX>(img, x0, y0, tab.D, tab.S, g, s_blob, tab.run_word, tab.weight_word, s_tab, s_tile);
+    sweep_tile<WX>(img, x0, y0, tab.D, tab.S, g, s_blob, tab.run_word, tab.weight_word, s_tab, s_tile,
+                   tab.neg_zero);
 }
 
 namespace {

@@ -47,6 +47,7 @@ struct ImageArgs {
 
 struct KernelTables {
     int D, S, R;
+    float neg_zero;  // -0.0f, read at run time (see prod2 in tile_core.cuh)
     const int *blob;  // device blob (BlobLayout)
     int blob_words, run_word, weight_word;
     float var[kMaxKernels];

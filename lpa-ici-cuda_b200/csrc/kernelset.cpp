@@ -141,6 +141,7 @@ void fill_tables(const lpaici_kernelset *ks, const float *var_or_null, float sig
     const int nk = ks->D * ks->S;
     t->D = ks->D;
     t->S = ks->S;
+    t->neg_zero = -0.0f;
     t->R = ks->radius;
     t->blob_words = ks->layout.total_words;
     t->run_word = ks->layout.run_word;

@@ -9,8 +9,8 @@
 //
 // Thread mapping: a warp covers 16 rows x 16 columns; lane = 4a + b owns the 8 pixels of rows
 // (a, a + 8) and columns 4b .. 4b + 3 of its warp's block, held as 4 float2 pairs {row a, row a+8}.
-// Every window value is then a natural register pair, so one packed __fmul2_rn / __fadd2_rn does two
-// pixels' taps.  A 16-lane half-warp's 8-byte loads hit 16 different bank pairs (pitch2 odd: the 4
+// Every window value is then a natural register pair, so one packed product and one packed add do
+// two pixels' taps.  A 16-lane half-warp's 8-byte loads hit 16 different bank pairs (pitch2 odd: the 4
 // rows give 4 residues mod 4, the column groups 4b the multiples of 4).
 //
 // Arithmetic (bit-identical to src/v1_0_lpa_ici_2D_fused.cpp:803-930 for finite inputs):
@@ -26,8 +26,33 @@
 
 namespace lpaici {
 
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+// Packed FP32 arithmetic, two lanes per instruction, each half rounded to nearest on its own.
+//
+// ptxas contracts a packed multiply feeding a packed add (mul.rn.f32x2 -> add.rn.f32x2) into one
+// fused multiply-add even with .rn and --fmad=false, which changes the rounding of the sums.  The
+// product is therefore formed as fma.rn.f32x2(w, x, nz) with nz = {-0, -0} passed in at run time
+// (so it cannot be folded away): w*x + (-0) is w*x exactly before the single rounding, hence the
+// correctly rounded product with its sign of zero; an fma feeding an add is never contracted.
+__device__ __forceinline__ float2 prod2(float2 a, float2 b, float2 nz) {
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
+        "fma.rn.f32x2 rd, ra, rb, rc;\n\t"
+        "mov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(nz.x), "f"(nz.y));
+    return d;
+}
+__device__ __forceinline__ float2 add2(float2 a, float2 b) {
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "add.rn.f32x2 rd, ra, rb;\n\t"
+        "mov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
 
 // Smallest odd pitch (in float2) >= need.
 __host__ __device__ inline int tile_pitch2(int need) { return need | 1; }
@@ -61,14 +86,14 @@ __host__ __device__ inline int table_words(int nk) { return (3 * nk + 3) & ~3; }
     {                                                                         \
         win[((J) + 3) & 3] = src[k + (J) + 3];                                \
         const float2 w2 = make_float2(WX_, WY_);                              \
-        _Pragma("unroll") for (int m = 0; m < 4; m++) acc[m] = add2(acc[m], mul2(w2, win[((J) + m) & 3])); \
+        _Pragma("unroll") for (int m = 0; m < 4; m++) acc[m] = add2(acc[m], prod2(w2, win[((J) + m) & 3], nz)); \
     }
 
 // acc[m] += sum_{j < len} {w_j, w_j} * src[m + j], tap by tap in order, for the 4 pixel pairs.
 // src: the run's first column in T8 (row already chosen); wq: the run's duplicated weights as
 // float4 {w_2i, w_2i, w_2i+1, w_2i+1}.
 __device__ __forceinline__ void conv_run(float2 (&acc)[4], const float2 *__restrict__ src,
-                                         const float4 *__restrict__ wq, int len) {
+                                         const float4 *__restrict__ wq, int len, float2 nz) {
     float2 win[4];
     win[0] = src[0];
     win[1] = src[1];
@@ -150,7 +175,7 @@ __device__ __forceinline__ float pick(const float2 (&v)[4], int i) { return (i &
 // ends when every pixel of the warp has stopped.
 __device__ __forceinline__ void direction_sweep(int d, int S, unsigned valid, const float2 *lane_tile, int pitch2,
                                                 const int *s_blob, const int4 *s_runs, const float4 *s_wq,
-                                                const float *s_thr, float (&best)[8], unsigned &sidx) {
+                                                const float *s_thr, float2 nz, float (&best)[8], unsigned &sidx) {
     float lo[8], hi[8];
 #pragma unroll
     for (int i = 0; i < 8; i++) {
@@ -169,7 +194,7 @@ __device__ __forceinline__ void direction_sweep(int d, int S, unsigned valid, co
         const int rb = s_blob[k], re = s_blob[k + 1];
         for (int r = rb; r < re; r++) {
             const int4 run = s_runs[r];
-            conv_run(acc, lane_tile + run.x * pitch2 + run.y, s_wq + (run.w >> 1), run.z);
+            conv_run(acc, lane_tile + run.x * pitch2 + run.y, s_wq + (run.w >> 1), run.z, nz);
         }
         const float thr = s_thr[k];
         float2 lb[4], ub[4];
@@ -198,7 +223,7 @@ __device__ __forceinline__ void direction_sweep(int d, int S, unsigned valid, co
 template <int WX>
 __device__ __forceinline__ void sweep_tile(const ImageArgs &img, int x0, int y0, int D, int S, const TileGeom &g,
                                            const int *s_blob, int run_word, int weight_word, const float *s_tab,
-                                           const float2 *s_tile) {
+                                           const float2 *s_tile, float neg_zero) {
     const LaneGeom<WX> lg;
     const int nk = D * S;
     const int oy = y0 + lg.ty, ox = x0 + lg.tx;
@@ -210,6 +235,7 @@ __device__ __forceinline__ void sweep_tile(const ImageArgs &img, int x0, int y0,
     const int4 *s_runs = reinterpret_cast<const int4 *>(s_blob + run_word);
     const float4 *s_wq = reinterpret_cast<const float4 *>(s_blob + weight_word);
     const float *s_thr = s_tab + nk, *s_rvar = s_tab + 2 * nk;
+    const float2 nz = make_float2(neg_zero, neg_zero);
 
     float2 num[4], den[4];
 #pragma unroll
@@ -218,12 +244,12 @@ __device__ __forceinline__ void sweep_tile(const ImageArgs &img, int x0, int y0,
     for (int d = 0; d < D; d++) {
         float best[8];
         unsigned sidx;
-        direction_sweep(d, S, valid, lane_tile, g.pitch2, s_blob, s_runs, s_wq, s_thr, best, sidx);
+        direction_sweep(d, S, valid, lane_tile, g.pitch2, s_blob, s_runs, s_wq, s_thr, nz, best, sidx);
 #pragma unroll
         for (int m = 0; m < 4; m++) {
             const float2 r = make_float2(s_rvar[d * S + ((sidx >> (8 * m)) & 15)],
                                          s_rvar[d * S + ((sidx >> (8 * m + 4)) & 15)]);
-            num[m] = add2(num[m], mul2(make_float2(best[2 * m], best[2 * m + 1]), r));
+            num[m] = add2(num[m], prod2(make_float2(best[2 * m], best[2 * m + 1]), r, nz));
             den[m] = add2(den[m], r);
         }
         if (img.smap) {
