@@ -11,9 +11,10 @@ rank's time.
             the launching stream), L2 flushed (256 MB write) between timed steps
   e2e       the same metric through the C ABI's host-pointer entry (lpaici_denoise_host): pinned host
             input -> H2D -> forward -> D2H -> host, synchronous, wall clock per step
-  roofline  FP32 issue bound: every tap is one multiply and one separately rounded add (bit-exact with
-            the reference), so the peak is the FP32 pipe's measured mul+add lane-op rate on this GPU
-            (probe in lib/liblpaici_bench.so); achieved = 2 x algorithmic taps / kernel time
+  roofline  FP32 bound: every tap is one multiply and one separately rounded add (bit-exact with the
+            reference), so the peak is the FP32 pipe's measured rate for exactly that (probe in
+            lib/liblpaici_bench.so, the faster of scalar FMUL+FADD and packed fma(w,x,-0)+add);
+            achieved = 2 x algorithmic taps / kernel time
   cpu_baseline  the reference's own CPU engine (anisotropic_lpa_ici_cpu_fused of
             src/v1_0_lpa_ici_2D_fused.cpp, compiled in-process into oracle/_ref/) on all host cores,
             one 256x256 crop of the benchmark image per thread
@@ -131,7 +132,7 @@ def fp32_peak() -> dict:
     r = (C.c_double * 3)()
     if lib.lpaici_bench_fp32_peak(r) != 0:
         raise RuntimeError("FP32 peak probe failed")
-    return {"ffma_lane_ops_per_s": r[0], "muladd_lane_ops_per_s": r[1], "muladd2_lane_ops_per_s": r[2]}
+    return {"ffma_ops_per_s": r[0], "muladd_ops_per_s": r[1], "prodadd2_ops_per_s": r[2]}
 
 
 def algorithmic_taps(torch, ks, smap) -> float:
@@ -342,7 +343,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
             torch.distributed.barrier()
         return
     kernel_s = ms_step * 1e-3
-    peak_ops = max(peak["muladd_lane_ops_per_s"], peak["muladd2_lane_ops_per_s"])
+    peak_ops = max(peak["muladd_ops_per_s"], peak["prodadd2_ops_per_s"])  # the exact forms only
     achieved = 2.0 * taps / kernel_s  # one multiply + one add per tap
     tw, th, thr, ppt = lpaici.tile_configs()[best]
     line = {
@@ -357,8 +358,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
                    "parallelism": f"dp{world} (independent images, no collective)"},
         "roofline": {"bound": "fp32", "achieved": achieved / 1e12, "peak": peak_ops / 1e12, "unit": "TFLOP/s",
                      "frac": achieved / peak_ops, "traffic": None,
-                     "note": "FLOP = 2 per algorithmic tap (mul + separately rounded add); peak = measured FP32 "
-                             "mul+add lane-op rate on this GPU",
+                     "note": "FLOP = 2 per algorithmic tap (multiply and add, each rounded: bit-exact with the "
+                             "reference); peak = the faster of the two exact FP32 forms measured live on this GPU "
+                             "(scalar FMUL+FADD, packed fma(w,x,-0)+add); scalar FFMA shown for context",
                      "algorithmic_taps_per_px": taps / px,
                      "fp32_probe_tops": {k: v / 1e12 for k, v in peak.items()}},
         "cpu_baseline": cpu,

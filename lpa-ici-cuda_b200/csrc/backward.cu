@@ -2,201 +2,151 @@
 //
 // For L = sum_p g[p] * out[p] and the selected scale s*(d,p) of every direction and pixel frozen,
 // out is linear in the input x:  out(p) = sum_d alpha_d(p) * sum_t h_{d,s*}(t) x(p + t - c), with
-// alpha_d(p) = (1/v_d(p)) / sum_d' (1/v_d'(p)).  Hence
-//     dL/dx(q) = sum_d sum_p g(p) * alpha_d(p) * h_{d,s*(d,p)}(q - p + c)      (zero padding).
-// One CTA per output tile, in three phases:
-//   1. recompute: the forward's exact ICI sweep over the input tile yields s*(d,p) for all 16
-//      directions (packed 4 bits per direction) and sum_d 1/v_d -- no scale map is stored or read;
-//   2. scatter: the input tile's shared memory becomes a gradient tile (tile + halo R); for every
-//      direction and every scale present in the warp, each thread spreads c_i = g_i * alpha_{d,i}
-//      (zero for pixels that selected another scale) through the kernel's row runs with a sliding
-//      window of 4 partial outputs per pixel row: 4 FMAs per weight, one shared-memory atomic per
-//      finished output;
-//   3. write-back: the gradient tile is added to the output with global atomics (halos of
-//      neighbouring tiles overlap).
+// alpha_d(p) = (1/v_d(p)) / den(p), den(p) = sum_d' 1/v_d'(p).  Hence, with c_d(p) = g(p) alpha_d(p),
+//     dL/dx(q) = sum_d sum_s sum_t h_{d,s}(t) [s*(d, q - t + c) = s] c_d(q - t + c)        (zero padding)
+// i.e. for every direction and scale, a correlation of the masked field c_d [s* = s] with the kernel
+// mirrored through its centre.  Two launches:
+//   A. selection: the forward's exact tile sweep recomputes s*(d,p) (one byte per direction and
+//      pixel) and den(p) into a transient workspace -- the forward stores nothing for the adjoint;
+//   B. gather: one CTA per output tile builds, per direction, c_d and s* on the tile plus its R-pixel
+//      halo in shared memory; per scale present there it masks the field and correlates it with the
+//      mirrored kernel's row runs (register sliding window, 9 outputs per thread, FFMA -- the adjoint
+//      is checked against FP64 finite differences, not bit patterns).  Every output is written once:
+//      no atomics, deterministic.
 // No counterpart in the reference.
 #include "configs.h"
 #include "tile_core.cuh"
 
 namespace lpaici {
 
-// dst[j] += sum_{i + k = j} c[i] * w_k for j < len + 3: the transpose of conv_run for one pixel row.
-// A window of 4 partial outputs slides along the run (slot j % 4 holds output j); every finished
-// output is added to shared memory with one atomic.  wq holds the run's duplicated weights.
-__device__ __forceinline__ void scatter_run(const float (&c)[4], float *dst, const float4 *__restrict__ wq, int len) {
-    float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-    const int n_out = len + 3;
-    for (int j0 = 0; j0 < n_out; j0 += 4) {
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const int j = j0 + q;
-            if (j < len) {  // taps of the run only (its weights are padded to an even count)
-                const float4 wp = wq[j >> 1];
-                const float w = (q & 1) ? wp.z : wp.x;
-#pragma unroll
-                for (int i = 0; i < 4; i++) acc[(i + q) & 3] = fmaf(c[i], w, acc[(i + q) & 3]);
-            }
-            if (j < n_out) {
-                atomicAdd(dst + j, acc[q]);
-                acc[q] = 0.0f;
-            }
-        }
-    }
-}
-
-template <int WX, int WY>
-__global__ void __launch_bounds__(32 * WX * WY, 1)
-    lpaici_backward_kernel(const __grid_constant__ ImageArgs img, const __grid_constant__ KernelTables tab) {
-    using Shape = TileShape<WX, WY>;
-    extern __shared__ __align__(16) int smem[];
-    const int D = tab.D, S = tab.S, nk = D * S;
-    int *s_blob = smem;
-    float *s_tab = reinterpret_cast<float *>(smem + tab.blob_words);
-    float2 *s_tile = reinterpret_cast<float2 *>(smem + tab.blob_words + table_words(nk));
-    float *s_grad = reinterpret_cast<float *>(s_tile);  // phase 2 reuses the tile's memory
-    const TileGeom g = TileGeom::make(Shape::kTileW, Shape::kTileH, tab.R);
-    const int R = g.R, gpitch = g.pitch2, grows = Shape::kTileH + 2 * R;
-    const int x0 = blockIdx.x * Shape::kTileW, y0 = blockIdx.y * Shape::kTileH;
-
-    stage_words(s_blob, tab.blob, tab.blob_words);
-    stage_tables(s_tab, tab.var, tab.thr, nk);
-    load_tile(s_tile, img, x0, y0, g);
-    __syncthreads();
-
-    const LaneGeom<WX> lg;
-    const int oy = y0 + lg.ty, ox = x0 + lg.tx;
-    unsigned valid = 0;
-#pragma unroll
-    for (int i = 0; i < 8; i++)
-        if (oy + 8 * (i & 1) < img.rows_out && ox + (i >> 1) < img.W) valid |= 1u << i;
-    const int4 *s_runs = reinterpret_cast<const int4 *>(s_blob + tab.run_word);
-    const float4 *s_wq = reinterpret_cast<const float4 *>(s_blob + tab.weight_word);
-    const float *s_thr = s_tab + nk, *s_rvar = s_tab + 2 * nk;
-
-    // phase 1: the selection of every direction (4 bits each) and sum_d 1/v_d, per pixel
-    unsigned long long sel[8];
-    float den[8];
-#pragma unroll
-    for (int i = 0; i < 8; i++) {
-        sel[i] = 0ull;
-        den[i] = 0.0f;
-    }
-    const float2 *lane_tile = s_tile + (lg.ty + R) * g.pitch2 + lg.tx + R;
-    for (int d = 0; d < D; d++) {
-        float best[8];
-        unsigned sidx;
-        direction_sweep(d, S, valid, lane_tile, g.pitch2, s_blob, s_runs, s_wq, s_thr,
-                        make_float2(tab.neg_zero, tab.neg_zero), best, sidx);
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-            const unsigned si = (sidx >> (4 * i)) & 15u;
-            sel[i] |= static_cast<unsigned long long>(si) << (4 * d);
-            den[i] += s_rvar[d * S + si];
-        }
-    }
-    __syncthreads();  // done reading the input tile
-
-    // phase 2: the tile's memory becomes the gradient accumulator (tile + R halo, plain floats)
-    for (int i = threadIdx.x; i < grows * gpitch; i += blockDim.x) s_grad[i] = 0.0f;
-    float gp[8];
-#pragma unroll
-    for (int i = 0; i < 8; i++)
-        gp[i] = (valid & (1u << i)) ? __ldg(img.gout + static_cast<size_t>(oy + 8 * (i & 1)) * img.gout_pitch + ox +
-                                            (i >> 1))
-                                    : 0.0f;
-    __syncthreads();
-
-    float *lane_grad = s_grad + (lg.ty + R) * gpitch + lg.tx + R;
-    for (int d = 0; d < D; d++) {
-        float c[8];
-        unsigned present = 0;
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-            const int s = static_cast<int>((sel[i] >> (4 * d)) & 15ull);
-            c[i] = (valid & (1u << i)) ? gp[i] * (s_rvar[d * S + s] / den[i]) : 0.0f;
-            if (valid & (1u << i)) present |= 1u << s;
-        }
-        present = __reduce_or_sync(0xffffffffu, present);
-        while (present) {
-            const int s = __ffs(present) - 1;
-            present &= present - 1;
-            float c0[4], c1[4];  // rows ty and ty + 8
-#pragma unroll
-            for (int m = 0; m < 4; m++) {
-                c0[m] = (static_cast<int>((sel[2 * m] >> (4 * d)) & 15ull) == s) ? c[2 * m] : 0.0f;
-                c1[m] = (static_cast<int>((sel[2 * m + 1] >> (4 * d)) & 15ull) == s) ? c[2 * m + 1] : 0.0f;
-            }
-            const int k = d * S + s;
-            const int rb = s_blob[k], re = s_blob[k + 1];
-            for (int r = rb; r < re; r++) {
-                const int4 run = s_runs[r];
-                float *dst = lane_grad + run.x * gpitch + run.y;
-                scatter_run(c0, dst, s_wq + (run.w >> 1), run.z);
-                scatter_run(c1, dst + 8 * gpitch, s_wq + (run.w >> 1), run.z);
-            }
-        }
-    }
-    __syncthreads();
-
-    // phase 3: add the gradient tile (with its halo) to the output
-    const int gy0 = y0 + img.row_begin - R, gx0 = x0 - R;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-    for (int r = warp; r < grows; r += nwarps) {
-        const int gy = gy0 + r;
-        if (gy < 0 || gy >= img.in_h) continue;
-        float *dst = img.out + static_cast<size_t>(gy) * img.out_pitch;
-        const float *src = s_grad + r * gpitch;
-        for (int cc = lane; cc < gpitch; cc += 32) {
-            const int gx = gx0 + cc;
-            if (gx >= 0 && gx < img.W) {
-                const float v = src[cc];
-                if (v != 0.0f) atomicAdd(dst + gx, v);
-            }
-        }
-    }
-}
-
 namespace {
 
-template <int WX, int WY>
-int launch_bwd(const ImageArgs &img, const KernelTables &tab, cudaStream_t stream) {
-    using Shape = TileShape<WX, WY>;
-    const TileGeom g = TileGeom::make(Shape::kTileW, Shape::kTileH, tab.R);
-    const int nk = tab.D * tab.S;
-    const size_t grad_bytes = sizeof(float) * static_cast<size_t>(g.pitch2) * (Shape::kTileH + 2 * tab.R);
-    const size_t region = g.tile_bytes() > grad_bytes ? g.tile_bytes() : grad_bytes;
-    const size_t smem = sizeof(int) * (tab.blob_words + table_words(nk)) + region;
-    auto kern = lpaici_backward_kernel<WX, WY>;
-    int dev = 0, max_optin = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    if (smem > static_cast<size_t>(max_optin))
-        return set_error(LPAICI_ERR_UNSUPPORTED, "backward tile needs %zu B of shared memory, device allows %d", smem,
-                         max_optin);
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute(backward)");
-    const dim3 grid((img.W + Shape::kTileW - 1) / Shape::kTileW, (img.rows_out + Shape::kTileH - 1) / Shape::kTileH);
-    if (grid.y > 65535u) return set_error(LPAICI_ERR_UNSUPPORTED, "image too tall: %d rows", img.rows_out);
-    kern<<<grid, Shape::kThreads, smem, stream>>>(img, tab);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_error(e, "backward launch");
-    return LPAICI_OK;
+constexpr int kGatherP = 9;  // outputs per thread (odd: conflict-free scalar shared loads)
+constexpr int kGatherWX = 2, kGatherWY = 8;
+constexpr int kGatherTW = kGatherWX * 4 * kGatherP, kGatherTH = kGatherWY * 8;  // 72 x 64, 512 threads
+
+struct GatherArgs {
+    const float *g;        // cotangent, pitch g_pitch
+    const uint8_t *smap;   // D x H x W selected scales (pass A)
+    const float *den;      // H x W, pitch W (pass A)
+    float *grad;           // result, pitch grad_pitch
+    int g_pitch, grad_pitch, W, H;
+    int D, S, R;
+    const int *blob;       // mirrored kernels (lpaici_kernelset::adj_blob)
+    int blob_words, run_word, weight_word;
+    int pitch, rows;       // shared-memory field geometry (floats)
+    float rvar[kMaxKernels];
+};
+
+// Smallest pitch >= need with (pitch / 4) odd: scalar loads of 8 rows x 4 column groups of 9 hit 32
+// different banks.
+__host__ __device__ inline int field_pitch(int need) {
+    int p = (need + 3) & ~3;
+    if (((p >> 2) & 1) == 0) p += 4;
+    return p;
+}
+
+// acc[i] += sum_{j < len} w[j] * src[i + j] for the thread's P outputs (sliding window, FFMA).
+template <int P>
+__device__ __forceinline__ void gather_run(float (&acc)[P], const float *__restrict__ src, const float *__restrict__ w,
+                                           int len) {
+    float win[P];
+#pragma unroll
+    for (int i = 0; i < P - 1; i++) win[i] = src[i];
+    int k = 0;
+    for (; k + P <= len; k += P) {
+#pragma unroll
+        for (int j = 0; j < P; j++) {
+            win[(j + P - 1) % P] = src[k + j + P - 1];
+            const float wt = w[k + j];
+#pragma unroll
+            for (int i = 0; i < P; i++) acc[i] = fmaf(wt, win[(j + i) % P], acc[i]);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < P - 1; j++) {
+        if (k + j < len) {
+            win[(j + P - 1) % P] = src[k + j + P - 1];
+            const float wt = w[k + j];
+#pragma unroll
+            for (int i = 0; i < P; i++) acc[i] = fmaf(wt, win[(j + i) % P], acc[i]);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(32 * kGatherWX * kGatherWY, 1)
+    lpaici_adjoint_gather_kernel(const __grid_constant__ GatherArgs a) {
+    constexpr int P = kGatherP;
+    extern __shared__ __align__(16) int smem[];
+    __shared__ unsigned s_present;
+    const int fsize = a.rows * a.pitch;
+    int *s_blob = smem;
+    float *s_c = reinterpret_cast<float *>(smem + a.blob_words);  // c_d on the halo'd tile
+    float *s_f = s_c + fsize;                                     // the masked field of one scale
+    uint8_t *s_s = reinterpret_cast<uint8_t *>(s_f + fsize);      // s*(d, .) on the halo'd tile
+    const int x0 = blockIdx.x * kGatherTW, y0 = blockIdx.y * kGatherTH;
+    const int gx0 = x0 - a.R, gy0 = y0 - a.R;
+
+    stage_words(s_blob, a.blob, a.blob_words);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    const int ty = (warp / kGatherWX) * 8 + (lane >> 2);
+    const int tx = (warp % kGatherWX) * 4 * P + (lane & 3) * P;
+    const int4 *s_runs = reinterpret_cast<const int4 *>(s_blob + a.run_word);
+    const float *s_w = reinterpret_cast<const float *>(s_blob + a.weight_word);
+    const float *lane_f = s_f + (ty + a.R) * a.pitch + tx + a.R;
+
+    float acc[P];
+#pragma unroll
+    for (int i = 0; i < P; i++) acc[i] = 0.0f;
+
+    for (int d = 0; d < a.D; d++) {
+        __syncthreads();  // the previous direction's gathers are done with the shared fields
+        if (threadIdx.x == 0) s_present = 0u;
+        __syncthreads();
+        unsigned present = 0;
+        const uint8_t *plane = a.smap + static_cast<size_t>(d) * a.H * a.W;
+        for (int r = warp; r < a.rows; r += nwarps) {  // one warp per row, lanes along it
+            const int gy = gy0 + r;
+            const bool row_ok = gy >= 0 && gy < a.H;
+            for (int cc = lane; cc < a.pitch; cc += 32) {
+                const int gx = gx0 + cc;
+                float c = 0.0f;
+                uint8_t s = 0xff;
+                if (row_ok && gx >= 0 && gx < a.W) {
+                    const size_t p = static_cast<size_t>(gy) * a.W + gx;
+                    s = plane[p];
+                    c = a.g[static_cast<size_t>(gy) * a.g_pitch + gx] * (a.rvar[d * a.S + s] / a.den[p]);
+                    present |= 1u << s;
+                }
+                s_c[r * a.pitch + cc] = c;
+                s_s[r * a.pitch + cc] = s;
+            }
+        }
+        atomicOr(&s_present, present);
+        __syncthreads();
+        const unsigned mask = s_present;
+        for (int s = 0; s < a.S; s++) {
+            if (!(mask & (1u << s))) continue;  // block-uniform
+            for (int i = threadIdx.x; i < fsize; i += blockDim.x) s_f[i] = (s_s[i] == s) ? s_c[i] : 0.0f;
+            __syncthreads();
+            const int k = d * a.S + s;
+            for (int r = s_blob[k]; r < s_blob[k + 1]; r++) {
+                const int4 run = s_runs[r];
+                gather_run<P>(acc, lane_f + run.x * a.pitch + run.y, s_w + run.w, run.z);
+            }
+            __syncthreads();  // before the next scale's field overwrites s_f
+        }
+    }
+    const int oy = y0 + ty;
+    if (oy < a.H) {
+        float *o = a.grad + static_cast<size_t>(oy) * a.grad_pitch + x0 + tx;
+#pragma unroll
+        for (int i = 0; i < P; i++)
+            if (x0 + tx + i < a.W) o[i] = acc[i];
+    }
 }
 
 }  // namespace
-
-#define LPAICI_BWD_CASE(idx, WX, WY) \
-    case idx: return launch_bwd<WX, WY>(img, tab, stream);
-
-int launch_backward(const lpaici_kernelset *ks, const ImageArgs &img, const KernelTables &tab, int config,
-                    cudaStream_t stream) {
-    (void)ks;
-    switch (config) {
-        LPAICI_TILE_CONFIGS(LPAICI_BWD_CASE)
-        default: return set_error(LPAICI_ERR_INVALID_ARG, "tile config %d out of range", config);
-    }
-}
-#undef LPAICI_BWD_CASE
 
 }  // namespace lpaici
 
@@ -211,28 +161,84 @@ extern "C" int lpaici_backward(const lpaici_kernelset *ks, const float *d_noisy,
         return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_backward: bad size or pitch");
     if (!(sigma > 0.0f) || !(gamma > 0.0f))
         return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_backward: sigma and gamma need positive numbers");
-    if (ks->D > 16 || ks->S > 16)
-        return set_error(LPAICI_ERR_UNSUPPORTED, "lpaici_backward supports at most 16 directions and 16 scales");
+    if (ks->S > 32) return set_error(LPAICI_ERR_UNSUPPORTED, "lpaici_backward supports at most 32 scales");
     cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
-    const int *blob = nullptr;
+    const int *blob = nullptr, *adj = nullptr;
     int rc = device_blob(ks, &blob);
+    if (rc == LPAICI_OK) rc = device_adj_blob(ks, &adj);
     if (rc != LPAICI_OK) return rc;
-    cudaError_t e = cudaMemset2DAsync(d_grad_in, sizeof(float) * gin_pitch, 0, sizeof(float) * width, height, stream);
-    if (e != cudaSuccess) return cuda_error(e, "cudaMemset2DAsync(grad)");
+
+    // pass B's shared memory: mirrored kernels + c_d, masked field (floats) + s* (bytes) on the tile + halo
+    GatherArgs ga{};
+    ga.R = ks->radius;
+    ga.pitch = field_pitch(kGatherTW + 2 * ga.R + kGatherP);
+    ga.rows = kGatherTH + 2 * ga.R;
+    ga.blob_words = static_cast<int>(ks->adj_blob.size());
+    const size_t fsize = static_cast<size_t>(ga.pitch) * ga.rows;
+    const size_t smem = sizeof(int) * ga.blob_words + 2 * sizeof(float) * fsize + fsize;
+    int dev = 0, max_optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (smem > static_cast<size_t>(max_optin))
+        return set_error(LPAICI_ERR_UNSUPPORTED, "adjoint tile needs %zu B of shared memory, device allows %d", smem,
+                         max_optin);
+
+    // transient workspace: D selection planes (bytes) and den (floats)
+    const size_t npx = static_cast<size_t>(width) * height;
+    void *ws = nullptr;
+    const size_t smap_bytes = (static_cast<size_t>(ks->D) * npx + 255) & ~size_t(255);
+    cudaError_t e = cudaMallocAsync(&ws, smap_bytes + sizeof(float) * npx, stream);
+    if (e != cudaSuccess) return cuda_error(e, "cudaMallocAsync(adjoint workspace)");
+    uint8_t *smap = static_cast<uint8_t *>(ws);
+    float *den = reinterpret_cast<float *>(static_cast<char *>(ws) + smap_bytes);
+
+    // A. selection
     ImageArgs img{};
     img.in = d_noisy;
-    img.out = d_grad_in;
-    img.gout = d_grad_out;
-    img.smap = nullptr;
+    img.out = nullptr;
+    img.smap = smap;
+    img.den = den;
     img.W = width;
     img.in_h = height;
     img.in_pitch = noisy_pitch;
-    img.out_pitch = gin_pitch;
-    img.gout_pitch = gout_pitch;
+    img.out_pitch = width;
     img.row_begin = 0;
     img.rows_out = height;
     KernelTables tab;
     fill_tables(ks, nullptr, sigma, gamma, &tab);
     tab.blob = blob;
-    return launch_backward(ks, img, tab, default_config(ks), stream);
+    rc = launch_forward(ks, img, tab, default_config(ks), stream);
+
+    // B. gather
+    if (rc == LPAICI_OK) {
+        ga.g = d_grad_out;
+        ga.smap = smap;
+        ga.den = den;
+        ga.grad = d_grad_in;
+        ga.g_pitch = gout_pitch;
+        ga.grad_pitch = gin_pitch;
+        ga.W = width;
+        ga.H = height;
+        ga.D = ks->D;
+        ga.S = ks->S;
+        ga.blob = adj;
+        ga.run_word = ks->adj_run_word;
+        ga.weight_word = ks->adj_weight_word;
+        for (int k = 0; k < ks->D * ks->S; k++) ga.rvar[k] = 1.0f / tab.var[k];
+        e = cudaFuncSetAttribute(lpaici_adjoint_gather_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem));
+        if (e == cudaSuccess) {
+            const dim3 grid((width + kGatherTW - 1) / kGatherTW, (height + kGatherTH - 1) / kGatherTH);
+            if (grid.y > 65535u) {
+                rc = set_error(LPAICI_ERR_UNSUPPORTED, "image too tall: %d rows", height);
+            } else {
+                lpaici_adjoint_gather_kernel<<<grid, 32 * kGatherWX * kGatherWY, smem, stream>>>(ga);
+                e = cudaGetLastError();
+            }
+        }
+        if (rc == LPAICI_OK && e != cudaSuccess) rc = cuda_error(e, "adjoint gather launch");
+    }
+    cudaError_t ef = cudaFreeAsync(ws, stream);
+    if (rc == LPAICI_OK && ef != cudaSuccess) rc = cuda_error(ef, "cudaFreeAsync(adjoint workspace)");
+    return rc;
 }

@@ -39,17 +39,17 @@ struct BatchArgs {
     float neg_zero;  // -0.0f, read at run time (see prod2 in tile_core.cuh)
 };
 
-template <int WX, int WY>
+template <int WX, int WY, int Q>
 __global__ void __launch_bounds__(32 * WX * WY, 1)
     lpaici_batched_kernel(const __grid_constant__ BatchArgs a) {
-    using Shape = TileShape<WX, WY>;
+    using Shape = TileShape<WX, WY, Q>;
     extern __shared__ __align__(16) int smem[];
     __shared__ int s_item;
     const int nk = a.D * a.S;
     int *s_blob = smem;
     float *s_tab = reinterpret_cast<float *>(smem + a.blob_words);
     float2 *s_tile = reinterpret_cast<float2 *>(smem + a.blob_words + table_words(nk));
-    const TileGeom g = TileGeom::make(Shape::kTileW, Shape::kTileH, a.R);
+    const TileGeom g = TileGeom::make(Shape::kTileW, Shape::kTileH, a.R, Q);
 
     stage_words(s_blob, a.blob, a.blob_words);
     int cur_image = -1;
@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(32 * WX * WY, 1)
         img.rows_out = bi.H;
         load_tile(s_tile, img, x0, y0, g);
         __syncthreads();
-        sweep_tile<WX>(img, x0, y0, a.D, a.S, g, s_blob, a.run_word, a.weight_word, s_tab, s_tile, a.neg_zero);
+        sweep_tile<WX, Q>(img, x0, y0, a.D, a.S, g, s_blob, a.run_word, a.weight_word, s_tab, s_tile, a.neg_zero);
         __syncthreads();  // everyone done with s_tile / s_item before the next tile
     }
 }
@@ -93,12 +93,12 @@ struct KernelInfo {
     size_t smem;
 };
 
-template <int WX, int WY>
+template <int WX, int WY, int Q>
 int batched_info(const KernelTables &tab, KernelInfo *info) {
-    using Shape = TileShape<WX, WY>;
-    const TileGeom g = TileGeom::make(Shape::kTileW, Shape::kTileH, tab.R);
+    using Shape = TileShape<WX, WY, Q>;
+    const TileGeom g = TileGeom::make(Shape::kTileW, Shape::kTileH, tab.R, Q);
     const int nk = tab.D * tab.S;
-    info->fn = reinterpret_cast<const void *>(lpaici_batched_kernel<WX, WY>);
+    info->fn = reinterpret_cast<const void *>(lpaici_batched_kernel<WX, WY, Q>);
     info->tile_w = Shape::kTileW;
     info->tile_h = Shape::kTileH;
     info->threads = Shape::kThreads;
@@ -107,8 +107,8 @@ int batched_info(const KernelTables &tab, KernelInfo *info) {
 }
 
 int get_info(int config, const KernelTables &tab, KernelInfo *info) {
-#define LPAICI_BATCH_CASE(idx, WX, WY) \
-    case idx: return batched_info<WX, WY>(tab, info);
+#define LPAICI_BATCH_CASE(idx, WX, WY, Q) \
+    case idx: return batched_info<WX, WY, Q>(tab, info);
     switch (config) {
         LPAICI_TILE_CONFIGS(LPAICI_BATCH_CASE)
         default: return set_error(LPAICI_ERR_INVALID_ARG, "tile config %d out of range", config);

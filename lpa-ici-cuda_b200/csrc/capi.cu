@@ -101,12 +101,12 @@ int lpaici_forward_rows(const lpaici_kernelset *ks, const float *d_in, int in_pi
 int lpaici_num_tile_configs(void) { return LPAICI_NUM_TILE_CONFIGS; }
 
 int lpaici_tile_config_desc(int index, int *tile_w, int *tile_h, int *threads, int *pixels_per_thread) {
-#define LPAICI_DESC_CASE(idx, WX, WY)                    \
-    case idx:                                            \
-        if (tile_w) *tile_w = (WX) * 16;                 \
-        if (tile_h) *tile_h = (WY) * 16;                 \
-        if (threads) *threads = 32 * (WX) * (WY);        \
-        if (pixels_per_thread) *pixels_per_thread = 8;   \
+#define LPAICI_DESC_CASE(idx, WX, WY, Q)                  \
+    case idx:                                             \
+        if (tile_w) *tile_w = (WX) * 4 * (Q);             \
+        if (tile_h) *tile_h = (WY) * 16;                  \
+        if (threads) *threads = 32 * (WX) * (WY);         \
+        if (pixels_per_thread) *pixels_per_thread = 2 * (Q); \
         return LPAICI_OK;
     switch (index) {
         LPAICI_TILE_CONFIGS(LPAICI_DESC_CASE)

@@ -11,35 +11,35 @@
 
 namespace lpaici {
 
-template <int WX, int WY>
+template <int WX, int WY, int Q>
 __global__ void __launch_bounds__(32 * WX * WY, 1)
     lpaici_forward_kernel(const __grid_constant__ ImageArgs img, const __grid_constant__ KernelTables tab) {
-    using Shape = TileShape<WX, WY>;
+    using Shape = TileShape<WX, WY, Q>;
     extern __shared__ __align__(16) int smem[];
     const int nk = tab.D * tab.S;
     int *s_blob = smem;
     float *s_tab = reinterpret_cast<float *>(smem + tab.blob_words);
     float2 *s_tile = reinterpret_cast<float2 *>(smem + tab.blob_words + table_words(nk));
-    const TileGeom g = TileGeom::make(Shape::kTileW, Shape::kTileH, tab.R);
+    const TileGeom g = TileGeom::make(Shape::kTileW, Shape::kTileH, tab.R, Q);
     const int x0 = blockIdx.x * Shape::kTileW, y0 = blockIdx.y * Shape::kTileH;
 
     stage_words(s_blob, tab.blob, tab.blob_words);
     stage_tables(s_tab, tab.var, tab.thr, nk);
     load_tile(s_tile, img, x0, y0, g);
     __syncthreads();
-    sweep_tile<WX>(img, x0, y0, tab.D, tab.S, g, s_blob, tab.run_word, tab.weight_word, s_tab, s_tile,
+    sweep_tile<WX, Q>(img, x0, y0, tab.D, tab.S, g, s_blob, tab.run_word, tab.weight_word, s_tab, s_tile,
                    tab.neg_zero);
 }
 
 namespace {
 
-template <int WX, int WY>
+template <int WX, int WY, int Q>
 int launch_cfg(const ImageArgs &img, const KernelTables &tab, cudaStream_t stream) {
-    using Shape = TileShape<WX, WY>;
-    const TileGeom g = TileGeom::make(Shape::kTileW, Shape::kTileH, tab.R);
+    using Shape = TileShape<WX, WY, Q>;
+    const TileGeom g = TileGeom::make(Shape::kTileW, Shape::kTileH, tab.R, Q);
     const int nk = tab.D * tab.S;
     const size_t smem = sizeof(int) * (tab.blob_words + table_words(nk)) + g.tile_bytes();
-    auto kern = lpaici_forward_kernel<WX, WY>;
+    auto kern = lpaici_forward_kernel<WX, WY, Q>;
     int dev = 0, max_optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
@@ -58,18 +58,15 @@ int launch_cfg(const ImageArgs &img, const KernelTables &tab, cudaStream_t strea
 
 }  // namespace
 
-#define LPAICI_FWD_CASE(idx, WX, WY) \
-    case idx: return launch_cfg<WX, WY>(img, tab, stream);
+#define LPAICI_FWD_CASE(idx, WX, WY, Q) \
+    case idx: return launch_cfg<WX, WY, Q>(img, tab, stream);
 
-// Shared memory a tile configuration needs for a kernel set: blob + tables + the larger of the
-// T8 tile (forward) and the plain gradient tile (adjoint).
+// Shared memory a tile configuration needs for a kernel set: blob + tables + the T8 tile.
 size_t config_smem(int config, int blob_words, int nk, int R) {
-#define LPAICI_SMEM_CASE(idx, WX, WY)                                                                  \
-    case idx: {                                                                                        \
-        const TileGeom g = TileGeom::make(16 * (WX), 16 * (WY), R);                                   \
-        const size_t grad = sizeof(float) * static_cast<size_t>(g.pitch2) * (16 * (WY) + 2 * R);       \
-        return sizeof(int) * (blob_words + table_words(nk)) + (g.tile_bytes() > grad ? g.tile_bytes() : grad); \
-    }
+#define LPAICI_SMEM_CASE(idx, WX, WY, Q)                                                   \
+    case idx:                                                                              \
+        return sizeof(int) * (blob_words + table_words(nk)) +                              \
+               TileGeom::make(4 * (Q) * (WX), 16 * (WY), R, Q).tile_bytes();
     switch (config) {
         LPAICI_TILE_CONFIGS(LPAICI_SMEM_CASE)
         default: return ~size_t(0);

@@ -38,8 +38,9 @@ struct BlobLayout {
 struct ImageArgs {
     const float *in;  // input rows [0, in_h), width W, pitch in_pitch
     float *out;       // output rows [0, rows_out), pitch out_pitch
-    const float *gout;  // backward only: cotangent, same geometry as out
+    const float *gout;  // adjoint gather only: cotangent, same geometry as out
     uint8_t *smap;    // optional D x rows_out x W scale map
+    float *den;       // optional rows_out x W map of sum_d 1/v_d (pitch W; the adjoint's selection pass)
     int W, in_h, in_pitch, out_pitch, gout_pitch;
     int row_begin;    // output row r is input row row_begin + r
     int rows_out;
@@ -75,9 +76,14 @@ struct lpaici_kernelset {
     int radius = 0;
     lpaici::BlobLayout layout;
     std::vector<int32_t> blob;  // host copy of the device blob
+    // the adjoint's flipped kernels (taps (-dy, -dx), weights reversed): [begin (nk+1)] [Run records
+    // {dy, dx0, len, weight index}] [float weights, 16 spare zeros]
+    int adj_run_word = 0, adj_weight_word = 0;
+    std::vector<int32_t> adj_blob;
     // device copies, one per CUDA device, created on first use
     mutable std::mutex mu;
     mutable std::vector<int *> dev_blob;
+    mutable std::vector<int *> dev_adj_blob;
     mutable std::vector<int> tuned_config;  // per device, -1 = not tuned
 };
 
@@ -85,6 +91,8 @@ namespace lpaici {
 
 // Device blob of ks on the current device (uploaded on first use).  Returns an LPAICI_* code.
 int device_blob(const lpaici_kernelset *ks, const int **out);
+// The adjoint's flipped-kernel blob on the current device (uploaded on first use).
+int device_adj_blob(const lpaici_kernelset *ks, const int **out);
 
 // Fills var/thr exactly as the reference: var = (sigma*sigma)*norm2, thr = gamma*sqrt(var).
 void fill_tables(const lpaici_kernelset *ks, const float *var_or_null, float sigma, float gamma, KernelTables *t);
@@ -92,9 +100,7 @@ void fill_tables(const lpaici_kernelset *ks, const float *var_or_null, float sig
 // Forward / backward launchers (forward.cu, backward.cu).
 int launch_forward(const lpaici_kernelset *ks, const ImageArgs &img, const KernelTables &tab, int config,
                    cudaStream_t stream);
-int launch_backward(const lpaici_kernelset *ks, const ImageArgs &img, const KernelTables &tab, int config,
-                    cudaStream_t stream);
-// Bytes of shared memory tile configuration `config` needs for a kernel set (forward and adjoint).
+// Bytes of shared memory tile configuration `config` needs for a kernel set.
 size_t config_smem(int config, int blob_words, int nk, int R);
 // The autotuned configuration of ks on the current device, else the first one that fits.
 int default_config(const lpaici_kernelset *ks);

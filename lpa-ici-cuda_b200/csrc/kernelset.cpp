@@ -91,7 +91,9 @@ static int finish_kernelset(lpaici_kernelset *ks) {
         n2 += (ks->run_len[r] + 1) & ~1;
     }
     L.n_wdup = n2;
-    L.total_words = (L.weight_word + 2 * n2 + 3) & ~3;
+    // 16 spare {0, 0} taps after the last run: the speculative tail loads of the kernels read up to
+    // 8 taps past a run's end
+    L.total_words = (L.weight_word + 2 * (n2 + 16) + 3) & ~3;
     ks->blob.assign(L.total_words, 0);
     for (int k = 0; k < nk; k++) ks->blob[k] = ks->k_first_run[k];
     ks->blob[nk] = L.n_runs;
@@ -108,6 +110,26 @@ static int finish_kernelset(lpaici_kernelset *ks) {
                 wd[2 * (wofs[r] + j) + 1] = ks->run_w[w + j];
             }
             w += ks->run_len[r];
+        }
+    }
+
+    // adjoint blob: every run mirrored through the kernel centre
+    ks->adj_run_word = (nk + 1 + 3) & ~3;
+    ks->adj_weight_word = ks->adj_run_word + 4 * L.n_runs;
+    const int n_taps = static_cast<int>(ks->run_w.size());
+    ks->adj_blob.assign((ks->adj_weight_word + n_taps + 16 + 3) & ~3, 0);
+    for (int k = 0; k <= nk; k++) ks->adj_blob[k] = ks->blob[k];
+    float *aw = reinterpret_cast<float *>(ks->adj_blob.data() + ks->adj_weight_word);
+    for (int k = 0; k < nk; k++) {
+        int w = ks->k_first_weight[k];
+        for (int r = ks->k_first_run[k]; r < ks->k_first_run[k] + ks->k_num_runs[k]; r++) {
+            const int len = ks->run_len[r];
+            ks->adj_blob[ks->adj_run_word + 4 * r + 0] = -ks->run_row[r];
+            ks->adj_blob[ks->adj_run_word + 4 * r + 1] = -(ks->run_col[r] + len - 1);
+            ks->adj_blob[ks->adj_run_word + 4 * r + 2] = len;
+            ks->adj_blob[ks->adj_run_word + 4 * r + 3] = w;
+            for (int j = 0; j < len; j++) aw[w + j] = ks->run_w[w + len - 1 - j];
+            w += len;
         }
     }
     return LPAICI_OK;
@@ -134,6 +156,27 @@ int device_blob(const lpaici_kernelset *ks, const int **out) {
         ks->dev_blob[dev] = p;
     }
     *out = ks->dev_blob[dev];
+    return LPAICI_OK;
+}
+
+int device_adj_blob(const lpaici_kernelset *ks, const int **out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_error(e, "cudaGetDevice");
+    std::lock_guard<std::mutex> lock(ks->mu);
+    if (static_cast<int>(ks->dev_adj_blob.size()) <= dev) ks->dev_adj_blob.resize(dev + 1, nullptr);
+    if (!ks->dev_adj_blob[dev]) {
+        int *p = nullptr;
+        e = cudaMalloc(&p, sizeof(int32_t) * ks->adj_blob.size());
+        if (e != cudaSuccess) return cuda_error(e, "cudaMalloc(adjoint kernel set)");
+        e = cudaMemcpy(p, ks->adj_blob.data(), sizeof(int32_t) * ks->adj_blob.size(), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            cudaFree(p);
+            return cuda_error(e, "cudaMemcpy(adjoint kernel set)");
+        }
+        ks->dev_adj_blob[dev] = p;
+    }
+    *out = ks->dev_adj_blob[dev];
     return LPAICI_OK;
 }
 
@@ -359,6 +402,11 @@ int lpaici_kernelset_destroy(lpaici_kernelset *ks) {
         if (ks->dev_blob[d]) {
             cudaSetDevice(static_cast<int>(d));
             cudaFree(ks->dev_blob[d]);
+        }
+    for (size_t d = 0; d < ks->dev_adj_blob.size(); d++)
+        if (ks->dev_adj_blob[d]) {
+            cudaSetDevice(static_cast<int>(d));
+            cudaFree(ks->dev_adj_blob[d]);
         }
     if (cur >= 0) cudaSetDevice(cur);
     cudaGetLastError();

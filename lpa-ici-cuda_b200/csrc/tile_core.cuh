@@ -7,11 +7,13 @@
 //          8 apart, j < TH - 8 + 2R, c < pitch2 (odd); input row j is output row j - R of the tile,
 //          input column c is output column c - R; zero outside the input
 //
-// Thread mapping: a warp covers 16 rows x 16 columns; lane = 4a + b owns the 8 pixels of rows
-// (a, a + 8) and columns 4b .. 4b + 3 of its warp's block, held as 4 float2 pairs {row a, row a+8}.
-// Every window value is then a natural register pair, so one packed product and one packed add do
-// two pixels' taps.  A 16-lane half-warp's 8-byte loads hit 16 different bank pairs (pitch2 odd: the 4
-// rows give 4 residues mod 4, the column groups 4b the multiples of 4).
+// Thread mapping (Q = column pairs per thread, 4 or 8): a warp covers 16 rows x 4Q columns; the lane
+// with row index a (0..7) and column group b (0..3) owns the 2Q pixels of rows (a, a + 8) and columns
+// Qb .. Qb + Q - 1, held as Q float2 pairs {row a, row a + 8}.  Every window value is then a natural
+// register pair, so one packed product and one packed add do two pixels' taps.  The 16 lanes of a
+// half-warp hit 16 different bank pairs with 8-byte loads (pitch2 odd): Q = 4 puts 4 rows x 4 groups
+// in a half-warp (rows give the residues mod 4, groups the multiples of 4), Q = 8 puts 8 rows x 2
+// groups (rows give 8 distinct values mod 16 that never differ by 8, groups add 0 or 8).
 //
 // Arithmetic (bit-identical to src/v1_0_lpa_ici_2D_fused.cpp:803-930 for finite inputs):
 //   conv  = sum over the kernel's taps in row-major order of w*x (rounded), added one by one with
@@ -57,20 +59,21 @@ __device__ __forceinline__ float2 add2(float2 a, float2 b) {
 // Smallest odd pitch (in float2) >= need.
 __host__ __device__ inline int tile_pitch2(int need) { return need | 1; }
 
-template <int WX, int WY>
+template <int WX, int WY, int Q>
 struct TileShape {
     static constexpr int kThreads = 32 * WX * WY;
-    static constexpr int kTileW = WX * 16;
+    static constexpr int kTileW = WX * 4 * Q;
     static constexpr int kTileH = WY * 16;
 };
 
-// Shared-memory geometry of a tile for radius R.
+// Shared-memory geometry of a tile for radius R and Q column pairs per thread: tile_w + 2R columns
+// of halo'd input plus Q spare columns read (never used) by conv_run's speculative tail loads.
 struct TileGeom {
     int R, pitch2, pairs;  // pairs: number of T8 rows
-    __host__ __device__ static TileGeom make(int tile_w, int tile_h, int R) {
+    __host__ __device__ static TileGeom make(int tile_w, int tile_h, int R, int Q) {
         TileGeom g;
         g.R = R;
-        g.pitch2 = tile_pitch2(tile_w + 2 * R);
+        g.pitch2 = tile_pitch2(tile_w + 2 * R + Q);
         g.pairs = tile_h - 8 + 2 * R;
         return g;
     }
@@ -80,41 +83,51 @@ struct TileGeom {
 // Words of shared memory before the tile: the blob, then var/thr/rvar (padded to 16 bytes).
 __host__ __device__ inline int table_words(int nk) { return (3 * nk + 3) & ~3; }
 
-// One tap column of the sliding window: win slot (j + 3) % 4 receives column k + j + 3, then the
-// 4 pixel pairs m accumulate w * column (k + j + m).
-#define LPAICI_STEP(J, WX_, WY_)                                              \
-    {                                                                         \
-        win[((J) + 3) & 3] = src[k + (J) + 3];                                \
-        const float2 w2 = make_float2(WX_, WY_);                              \
-        _Pragma("unroll") for (int m = 0; m < 4; m++) acc[m] = add2(acc[m], prod2(w2, win[((J) + m) & 3], nz)); \
+// One tap column J of a block of Q: window slot (J + Q - 1) % Q receives column k + J + Q - 1, then
+// the Q pixel pairs m accumulate w * column (k + J + m).  Weights come two taps per float4.
+#define LPAICI_STEP(J)                                                                               \
+    {                                                                                                \
+        if (((J) & 1) == 0) wv = wq[(k + (J)) >> 1];                                                 \
+        const float2 w2 = ((J) & 1) ? make_float2(wv.z, wv.w) : make_float2(wv.x, wv.y);             \
+        win[((J) + Q - 1) % Q] = src[k + (J) + Q - 1];                                               \
+        _Pragma("unroll") for (int m = 0; m < Q; m++) acc[m] = add2(acc[m], prod2(w2, win[((J) + m) % Q], nz)); \
     }
 
-// acc[m] += sum_{j < len} {w_j, w_j} * src[m + j], tap by tap in order, for the 4 pixel pairs.
+// acc[m] += sum_{j < len} {w_j, w_j} * src[m + j], tap by tap in order, for the Q pixel pairs.
 // src: the run's first column in T8 (row already chosen); wq: the run's duplicated weights as
 // float4 {w_2i, w_2i, w_2i+1, w_2i+1}.
-__device__ __forceinline__ void conv_run(float2 (&acc)[4], const float2 *__restrict__ src,
+// The last len % Q taps: their window columns and weights are loaded before any of them is used --
+// unconditionally, which stays inside the tile (pitch2 carries Q spare columns) and the blob (the
+// weights carry spare taps) -- and only the arithmetic of each tap is guarded, so the tail pays no
+// load latency per tap.
+template <int Q>
+__device__ __forceinline__ void conv_run(float2 (&acc)[Q], const float2 *__restrict__ src,
                                          const float4 *__restrict__ wq, int len, float2 nz) {
-    float2 win[4];
-    win[0] = src[0];
-    win[1] = src[1];
-    win[2] = src[2];
+    float2 win[Q];
+    float4 wv;
+#pragma unroll
+    for (int i = 0; i < Q - 1; i++) win[i] = src[i];
     int k = 0;
-    for (; k + 4 <= len; k += 4) {
-        const float4 wa = wq[k >> 1], wb = wq[(k >> 1) + 1];
-        LPAICI_STEP(0, wa.x, wa.y)
-        LPAICI_STEP(1, wa.z, wa.w)
-        LPAICI_STEP(2, wb.x, wb.y)
-        LPAICI_STEP(3, wb.z, wb.w)
+    for (; k + Q <= len; k += Q) {
+#pragma unroll
+        for (int J = 0; J < Q; J++) LPAICI_STEP(J)
     }
-    const int rem = len - k;  // 0..3, warp-uniform
+    const int rem = len - k;  // 0 .. Q-1, warp-uniform
     if (rem > 0) {
-        const float4 wa = wq[k >> 1];
-        LPAICI_STEP(0, wa.x, wa.y)
-        if (rem > 1) {
-            LPAICI_STEP(1, wa.z, wa.w)
-            if (rem > 2) {
-                const float4 wb = wq[(k >> 1) + 1];  // the second tap of this float4 is padding
-                LPAICI_STEP(2, wb.x, wb.y)
+        float2 tail[Q - 1];
+        float4 tw[Q / 2];
+#pragma unroll
+        for (int J = 0; J < Q - 1; J++) tail[J] = src[k + J + Q - 1];
+#pragma unroll
+        for (int i = 0; i < Q / 2; i++) tw[i] = wq[(k >> 1) + i];
+#pragma unroll
+        for (int J = 0; J < Q - 1; J++) {
+            if (J < rem) {
+                const float2 w2 = (J & 1) ? make_float2(tw[J >> 1].z, tw[J >> 1].w)
+                                          : make_float2(tw[J >> 1].x, tw[J >> 1].y);
+                win[(J + Q - 1) % Q] = tail[J];
+#pragma unroll
+                for (int m = 0; m < Q; m++) acc[m] = add2(acc[m], prod2(w2, win[(J + m) % Q], nz));
             }
         }
     }
@@ -156,29 +169,33 @@ __device__ __forceinline__ void load_tile(float2 *s_tile, const ImageArgs &img, 
     }
 }
 
-// Lane geometry inside the tile: rows ty and ty + 8, columns tx .. tx + 3 (tile-local output).
-template <int WX>
+// Lane geometry inside the tile: rows ty and ty + 8, columns tx .. tx + Q - 1 (tile-local output).
+template <int WX, int Q>
 struct LaneGeom {
     int ty, tx;
     __device__ __forceinline__ LaneGeom() {
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        ty = (warp / WX) * 16 + (lane >> 2);
-        tx = (warp % WX) * 16 + (lane & 3) * 4;
+        const int a = Q == 4 ? (lane >> 2) : (lane & 7), b = Q == 4 ? (lane & 3) : (lane >> 3);
+        ty = (warp / WX) * 16 + a;
+        tx = (warp % WX) * 4 * Q + Q * b;
     }
 };
 
 // Pixel i = 2m + h of a thread: column tx + m, row ty + 8h.
-__device__ __forceinline__ float pick(const float2 (&v)[4], int i) { return (i & 1) ? v[i >> 1].y : v[i >> 1].x; }
+template <int Q>
+__device__ __forceinline__ float pick(const float2 (&v)[Q], int i) { return (i & 1) ? v[i >> 1].y : v[i >> 1].x; }
 
-// The ICI scale sweep of direction d for the thread's 8 pixels (mask `valid`): estimate and index
-// of the last accepted scale of every pixel (sidx: 4 bits per pixel).  Warp-uniform scale loop; it
-// ends when every pixel of the warp has stopped.
+// The ICI scale sweep of direction d for the thread's 2Q pixels (mask `valid`): estimate and index of
+// the last accepted scale of every pixel (sidx: 4 bits per pixel).  Warp-uniform scale loop; it ends
+// when every pixel of the warp has stopped.
+template <int Q>
 __device__ __forceinline__ void direction_sweep(int d, int S, unsigned valid, const float2 *lane_tile, int pitch2,
                                                 const int *s_blob, const int4 *s_runs, const float4 *s_wq,
-                                                const float *s_thr, float2 nz, float (&best)[8], unsigned &sidx) {
-    float lo[8], hi[8];
+                                                const float *s_thr, float2 nz, float (&best)[2 * Q],
+                                                unsigned long long &sidx) {
+    float lo[2 * Q], hi[2 * Q];
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
+    for (int i = 0; i < 2 * Q; i++) {
         lo[i] = -INFINITY;
         hi[i] = INFINITY;
         best[i] = 0.0f;
@@ -188,29 +205,29 @@ __device__ __forceinline__ void direction_sweep(int d, int S, unsigned valid, co
     for (int s = 0; s < S; s++) {
         if (!__any_sync(0xffffffffu, alive)) break;  // every pixel of the warp has stopped
         const int k = d * S + s;
-        float2 acc[4];
+        float2 acc[Q];
 #pragma unroll
-        for (int m = 0; m < 4; m++) acc[m] = make_float2(0.0f, 0.0f);
+        for (int m = 0; m < Q; m++) acc[m] = make_float2(0.0f, 0.0f);
         const int rb = s_blob[k], re = s_blob[k + 1];
         for (int r = rb; r < re; r++) {
             const int4 run = s_runs[r];
-            conv_run(acc, lane_tile + run.x * pitch2 + run.y, s_wq + (run.w >> 1), run.z, nz);
+            conv_run<Q>(acc, lane_tile + run.x * pitch2 + run.y, s_wq + (run.w >> 1), run.z, nz);
         }
         const float thr = s_thr[k];
-        float2 lb[4], ub[4];
+        float2 lb[Q], ub[Q];
 #pragma unroll
-        for (int m = 0; m < 4; m++) {
+        for (int m = 0; m < Q; m++) {
             lb[m] = add2(acc[m], make_float2(-thr, -thr));  // conv - thr, exactly
             ub[m] = add2(acc[m], make_float2(thr, thr));
         }
 #pragma unroll
-        for (int i = 0; i < 8; i++) {
+        for (int i = 0; i < 2 * Q; i++) {
             if (alive & (1u << i)) {
-                lo[i] = fmaxf(lo[i], pick(lb, i));
-                hi[i] = fminf(hi[i], pick(ub, i));
+                lo[i] = fmaxf(lo[i], pick<Q>(lb, i));
+                hi[i] = fminf(hi[i], pick<Q>(ub, i));
                 if (hi[i] >= lo[i]) {
-                    best[i] = pick(acc, i);
-                    sidx = (sidx & ~(15u << (4 * i))) | (static_cast<unsigned>(s) << (4 * i));
+                    best[i] = pick<Q>(acc, i);
+                    sidx = (sidx & ~(15ull << (4 * i))) | (static_cast<unsigned long long>(s) << (4 * i));
                 } else {
                     alive &= ~(1u << i);
                 }
@@ -220,16 +237,16 @@ __device__ __forceinline__ void direction_sweep(int d, int S, unsigned valid, co
 }
 
 // The forward sweep of one tile (tile in shared memory, block-synchronised).
-template <int WX>
+template <int WX, int Q>
 __device__ __forceinline__ void sweep_tile(const ImageArgs &img, int x0, int y0, int D, int S, const TileGeom &g,
                                            const int *s_blob, int run_word, int weight_word, const float *s_tab,
                                            const float2 *s_tile, float neg_zero) {
-    const LaneGeom<WX> lg;
+    const LaneGeom<WX, Q> lg;
     const int nk = D * S;
     const int oy = y0 + lg.ty, ox = x0 + lg.tx;
     unsigned valid = 0;
 #pragma unroll
-    for (int i = 0; i < 8; i++)
+    for (int i = 0; i < 2 * Q; i++)
         if (oy + 8 * (i & 1) < img.rows_out && ox + (i >> 1) < img.W) valid |= 1u << i;
     const float2 *lane_tile = s_tile + (lg.ty + g.R) * g.pitch2 + lg.tx + g.R;
     const int4 *s_runs = reinterpret_cast<const int4 *>(s_blob + run_word);
@@ -237,34 +254,42 @@ __device__ __forceinline__ void sweep_tile(const ImageArgs &img, int x0, int y0,
     const float *s_thr = s_tab + nk, *s_rvar = s_tab + 2 * nk;
     const float2 nz = make_float2(neg_zero, neg_zero);
 
-    float2 num[4], den[4];
+    float2 num[Q], den[Q];
 #pragma unroll
-    for (int m = 0; m < 4; m++) num[m] = den[m] = make_float2(0.0f, 0.0f);
+    for (int m = 0; m < Q; m++) num[m] = den[m] = make_float2(0.0f, 0.0f);
 
     for (int d = 0; d < D; d++) {
-        float best[8];
-        unsigned sidx;
-        direction_sweep(d, S, valid, lane_tile, g.pitch2, s_blob, s_runs, s_wq, s_thr, nz, best, sidx);
+        float best[2 * Q];
+        unsigned long long sidx;
+        direction_sweep<Q>(d, S, valid, lane_tile, g.pitch2, s_blob, s_runs, s_wq, s_thr, nz, best, sidx);
 #pragma unroll
-        for (int m = 0; m < 4; m++) {
-            const float2 r = make_float2(s_rvar[d * S + ((sidx >> (8 * m)) & 15)],
-                                         s_rvar[d * S + ((sidx >> (8 * m + 4)) & 15)]);
+        for (int m = 0; m < Q; m++) {
+            const float2 r = make_float2(s_rvar[d * S + static_cast<int>((sidx >> (8 * m)) & 15)],
+                                         s_rvar[d * S + static_cast<int>((sidx >> (8 * m + 4)) & 15)]);
             num[m] = add2(num[m], prod2(make_float2(best[2 * m], best[2 * m + 1]), r, nz));
             den[m] = add2(den[m], r);
         }
         if (img.smap) {
 #pragma unroll
-            for (int i = 0; i < 8; i++)
+            for (int i = 0; i < 2 * Q; i++)
                 if (valid & (1u << i))
                     img.smap[(static_cast<size_t>(d) * img.rows_out + oy + 8 * (i & 1)) * img.W + ox + (i >> 1)] =
                         static_cast<uint8_t>((sidx >> (4 * i)) & 15);
         }
     }
+    if (img.out) {
 #pragma unroll
-    for (int i = 0; i < 8; i++)
-        if (valid & (1u << i))
-            img.out[static_cast<size_t>(oy + 8 * (i & 1)) * img.out_pitch + ox + (i >> 1)] =
-                __fdiv_rn(pick(num, i), pick(den, i));
+        for (int i = 0; i < 2 * Q; i++)
+            if (valid & (1u << i))
+                img.out[static_cast<size_t>(oy + 8 * (i & 1)) * img.out_pitch + ox + (i >> 1)] =
+                    __fdiv_rn(pick<Q>(num, i), pick<Q>(den, i));
+    }
+    if (img.den) {
+#pragma unroll
+        for (int i = 0; i < 2 * Q; i++)
+            if (valid & (1u << i))
+                img.den[static_cast<size_t>(oy + 8 * (i & 1)) * img.W + ox + (i >> 1)] = pick<Q>(den, i);
+    }
 }
 
 }  // namespace lpaici
