@@ -174,12 +174,36 @@ int lpaici_set_tile_config(lpaici_kernelset *ks, int config);
 
 /* Gradient of L = sum_p g[p] * denoised[p] with respect to the noisy input, the ICI-selected scales
  * held fixed: grad[q] = sum_d sum_p g[p] * alpha_d(p) * h_{d,s*(d,p)}(q - p + c), with
- * alpha_d(p) = (1/v_d(p)) / sum_d' (1/v_d'(p)).  The scale maps are recomputed by a forward sweep
- * inside the launch, not read from memory.  No counterpart in the reference.
+ * alpha_d(p) = (1/v_d(p)) / sum_d' (1/v_d'(p)).  The selected scales and den are recomputed by an
+ * exact forward sweep into a transient workspace (D*width*height bytes + 4*width*height bytes, taken
+ * with cudaMallocAsync on `stream` and released stream-ordered); the forward keeps nothing for the
+ * adjoint.  No counterpart in the reference.
  *   d_grad_out  g, width x height (pitch gout_pitch);  d_grad_in  width x height (pitch gin_pitch) */
 int lpaici_backward(const lpaici_kernelset *ks, const float *d_noisy, int noisy_pitch, const float *d_grad_out,
                     int gout_pitch, float *d_grad_in, int gin_pitch, int width, int height, float sigma,
                     float gamma, lpaici_stream_t stream);
+
+/* Size of the static device scratch behind lpaici_backward_noalloc: 64 MiB per device. */
+#define LPAICI_NOALLOC_SCRATCH_BYTES (64u << 20)
+
+/* lpaici_backward without any device allocation: same arguments and result (same kernels, so equal to
+ * it), with its workspace and both kernel blobs in one file-scope __device__ array of
+ * LPAICI_NOALLOC_SCRATCH_BYTES instead of cudaMallocAsync / cudaMalloc.  For callers that cannot
+ * allocate device memory during a step: a framework whose caching allocator already holds the free
+ * memory, a loop that must not allocate after its setup, a device without stream-ordered memory
+ * pools.  No counterpart in the reference.
+ *   - Size limit: 256-byte-rounded (blob + mirrored blob + D*width*height bytes) + 4*width*height bytes
+ *     must fit the scratch (with 16 directions about 3.3 Mpx, e.g. 1920 x 1080); larger images return
+ *     LPAICI_ERR_UNSUPPORTED before any CUDA call.
+ *   - Nothing has to start at zero: every call copies the blobs in (host to device on `stream`) and
+ *     the selection sweep writes every byte the gather reads.
+ *   - The first call on each device looks up the array's address with cudaGetSymbolAddress, which
+ *     can load the module holding it; a caller that captures streams makes that first call before.
+ *   - One scratch per device: calls that overlap on one device (different streams or threads with
+ *     work in flight at once) race on it.  Serialise them, e.g. on one stream. */
+int lpaici_backward_noalloc(const lpaici_kernelset *ks, const float *d_noisy, int noisy_pitch,
+                            const float *d_grad_out, int gout_pitch, float *d_grad_in, int gin_pitch, int width,
+                            int height, float sigma, float gamma, lpaici_stream_t stream);
 
 /* ---- host-pointer entry points ---------------------------------------------------------------- */
 

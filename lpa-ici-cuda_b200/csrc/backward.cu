@@ -242,3 +242,63 @@ extern "C" int lpaici_backward(const lpaici_kernelset *ks, const float *d_noisy,
     if (rc == LPAICI_OK && ef != cudaSuccess) rc = cuda_error(ef, "cudaFreeAsync(adjoint workspace)");
     return rc;
 }
+
+// The same two passes as lpaici_backward, over caller-provided storage (lpaici_backward_noalloc).
+int lpaici::adjoint_passes(const lpaici_kernelset *ks, const int *blob, const int *adj_blob, uint8_t *smap,
+                           float *den, const float *d_noisy, int noisy_pitch, const float *d_grad_out,
+                           int gout_pitch, float *d_grad_in, int gin_pitch, int width, int height, float sigma,
+                           float gamma, cudaStream_t stream) {
+    GatherArgs ga{};
+    ga.R = ks->radius;
+    ga.pitch = field_pitch(kGatherTW + 2 * ga.R + kGatherP);
+    ga.rows = kGatherTH + 2 * ga.R;
+    ga.blob_words = static_cast<int>(ks->adj_blob.size());
+    const size_t fsize = static_cast<size_t>(ga.pitch) * ga.rows;
+    const size_t smem = sizeof(int) * ga.blob_words + 2 * sizeof(float) * fsize + fsize;
+    int dev = 0, max_optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (smem > static_cast<size_t>(max_optin))
+        return set_error(LPAICI_ERR_UNSUPPORTED, "adjoint tile needs %zu B of shared memory, device allows %d", smem,
+                         max_optin);
+    const dim3 grid((width + kGatherTW - 1) / kGatherTW, (height + kGatherTH - 1) / kGatherTH);
+    if (grid.y > 65535u) return set_error(LPAICI_ERR_UNSUPPORTED, "image too tall: %d rows", height);
+
+    ImageArgs img{};
+    img.in = d_noisy;
+    img.out = nullptr;
+    img.smap = smap;
+    img.den = den;
+    img.W = width;
+    img.in_h = height;
+    img.in_pitch = noisy_pitch;
+    img.out_pitch = width;
+    img.row_begin = 0;
+    img.rows_out = height;
+    KernelTables tab;
+    fill_tables(ks, nullptr, sigma, gamma, &tab);
+    tab.blob = blob;
+    int rc = launch_forward(ks, img, tab, default_config(ks), stream);
+    if (rc != LPAICI_OK) return rc;
+
+    ga.g = d_grad_out;
+    ga.smap = smap;
+    ga.den = den;
+    ga.grad = d_grad_in;
+    ga.g_pitch = gout_pitch;
+    ga.grad_pitch = gin_pitch;
+    ga.W = width;
+    ga.H = height;
+    ga.D = ks->D;
+    ga.S = ks->S;
+    ga.blob = adj_blob;
+    ga.run_word = ks->adj_run_word;
+    ga.weight_word = ks->adj_weight_word;
+    for (int k = 0; k < ks->D * ks->S; k++) ga.rvar[k] = 1.0f / tab.var[k];
+    cudaError_t e = cudaFuncSetAttribute(lpaici_adjoint_gather_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return cuda_error(e, "adjoint gather attributes");
+    lpaici_adjoint_gather_kernel<<<grid, 32 * kGatherWX * kGatherWY, smem, stream>>>(ga);
+    e = cudaGetLastError();
+    return e == cudaSuccess ? LPAICI_OK : cuda_error(e, "adjoint gather launch");
+}

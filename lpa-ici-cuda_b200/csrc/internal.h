@@ -104,5 +104,10 @@ int launch_forward(const lpaici_kernelset *ks, const ImageArgs &img, const Kerne
 size_t config_smem(int config, int blob_words, int nk, int R);
 // The autotuned configuration of ks on the current device, else the first one that fits.
 int default_config(const lpaici_kernelset *ks);
+// The adjoint's two passes over storage the caller provides: device copies of ks->blob and ks->adj_blob,
+// D*width*height selection bytes and width*height floats of den.  Allocates nothing.
+int adjoint_passes(const lpaici_kernelset *ks, const int *blob, const int *adj_blob, uint8_t *smap, float *den,
+                   const float *d_noisy, int noisy_pitch, const float *d_grad_out, int gout_pitch, float *d_grad_in,
+                   int gin_pitch, int width, int height, float sigma, float gamma, cudaStream_t stream);
 
 }  // namespace lpaici
