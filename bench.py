@@ -460,6 +460,36 @@ def run_extras(torch, lpaici, ks, args, flush) -> dict:
     }
 
 
+def run_profile(args) -> None:
+    """One operation on one synthetic size x size image, warmup + steps times, for profiler captures
+    (no bench line)."""
+    import torch
+
+    import lpaici
+
+    tmp = tempfile.mkdtemp()
+    ks = lpaici.KernelSet.load(kernel_path(SYM, tmp))
+    shutil.rmtree(tmp, ignore_errors=True)
+    if args.tile_config >= 0:
+        ks.set_tile_config(args.tile_config)
+    _, noisy_h = bench_image(args.size, SEED, SIGMA)
+    x = torch.from_numpy(noisy_h).cuda()
+    out = torch.empty_like(x)
+    g = torch.randn(args.size, args.size, generator=torch.Generator().manual_seed(0)).cuda()
+    ops = {"forward": lambda: lpaici.forward(ks, x, SIGMA, GAMMA, out=out),
+           "adjoint": lambda: lpaici.backward(ks, x, g, SIGMA, GAMMA, grad_in=out)}
+    op = ops[args.profile]
+    for _ in range(args.warmup):
+        op()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        op()
+    torch.cuda.synchronize()
+    print(json.dumps({"profile": args.profile, "size": args.size, "steps": args.steps,
+                      "ms_per_step_wall": (time.perf_counter() - t0) * 1e3 / max(1, args.steps)}))
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -472,12 +502,17 @@ def main():
     ap.add_argument("--no-parity", action="store_true")
     ap.add_argument("--size", type=int, default=SIZE, help="image side (profiling runs use a smaller case)")
     ap.add_argument("--tile-config", type=int, default=-1, help="fixed tile configuration instead of autotuning")
+    ap.add_argument("--profile", choices=["forward", "adjoint"], default=None,
+                    help="run only this operation on one --size image (for profiler captures; no bench line)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.profile:
+        run_profile(args)
         return
     if world > 1:
         import torch

@@ -3,9 +3,9 @@
 // cudaMalloc, cudaMallocAsync or memory pool; no torch).
 //
 // Scratch layout (each part starts on a 256-byte boundary):
-//   [forward kernel blob | mirrored kernel blob | D*W*H selection bytes | W*H floats of den]
+//   [forward kernel blob | mirrored kernel blob | D*W*H selection bytes | W*H floats of 1/den]
 // Nothing in it needs to start at zero: the two blobs are copied in by every call, pass A writes every
-// selection byte and den value that pass B reads.
+// selection byte and 1/den value that pass B reads.
 //
 // The array lives in its own translation unit, so the module that holds it is loaded only by callers of
 // this entry point.  No counterpart in the reference.
@@ -77,13 +77,13 @@ extern "C" int lpaici_backward_noalloc(const lpaici_kernelset *ks, const float *
     int *blob = reinterpret_cast<int *>(base);
     int *adj = reinterpret_cast<int *>(base + blob_bytes);
     uint8_t *smap = base + blob_bytes + adj_bytes;
-    float *den = reinterpret_cast<float *>(base + blob_bytes + adj_bytes + smap_bytes);
+    float *rden = reinterpret_cast<float *>(base + blob_bytes + adj_bytes + smap_bytes);
     cudaError_t e = cudaMemcpyAsync(blob, ks->blob.data(), sizeof(int) * ks->blob.size(), cudaMemcpyHostToDevice,
                                     stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(adj, ks->adj_blob.data(), sizeof(int) * ks->adj_blob.size(), cudaMemcpyHostToDevice,
                             stream);
     if (e != cudaSuccess) return cuda_error(e, "lpaici_backward_noalloc: kernel blobs to scratch");
-    return adjoint_passes(ks, blob, adj, smap, den, d_noisy, noisy_pitch, d_grad_out, gout_pitch, d_grad_in, gin_pitch,
+    return adjoint_passes(ks, blob, adj, smap, rden, d_noisy, noisy_pitch, d_grad_out, gout_pitch, d_grad_in, gin_pitch,
                           width, height, sigma, gamma, stream);
 }

@@ -70,7 +70,6 @@ __global__ void __launch_bounds__(32 * WX * WY, 1)
         ImageArgs img{};
         img.in = bi.in;
         img.out = bi.out;
-        img.gout = nullptr;
         img.smap = bi.smap;
         img.W = bi.W;
         img.in_h = bi.H;

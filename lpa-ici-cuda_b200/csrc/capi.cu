@@ -57,13 +57,11 @@ static int forward_common(const lpaici_kernelset *ks, const float *d_in, int in_
     ImageArgs img{};
     img.in = d_in;
     img.out = d_out;
-    img.gout = nullptr;
     img.smap = d_smap;
     img.W = width;
     img.in_h = in_height;
     img.in_pitch = in_pitch;
     img.out_pitch = out_pitch;
-    img.gout_pitch = 0;
     img.row_begin = row_begin;
     img.rows_out = row_count;
     KernelTables tab;

@@ -37,11 +37,10 @@ struct BlobLayout {
 // __grid_constant__ parameter; the tables are read with uniform indices from the constant bank).
 struct ImageArgs {
     const float *in;  // input rows [0, in_h), width W, pitch in_pitch
-    float *out;       // output rows [0, rows_out), pitch out_pitch
-    const float *gout;  // adjoint gather only: cotangent, same geometry as out
+    float *out;       // optional output rows [0, rows_out), pitch out_pitch
     uint8_t *smap;    // optional D x rows_out x W scale map
-    float *den;       // optional rows_out x W map of sum_d 1/v_d (pitch W; the adjoint's selection pass)
-    int W, in_h, in_pitch, out_pitch, gout_pitch;
+    float *rden;      // optional rows_out x W map of 1 / sum_d 1/v_d (pitch W; the adjoint's selection pass)
+    int W, in_h, in_pitch, out_pitch;
     int row_begin;    // output row r is input row row_begin + r
     int rows_out;
 };
@@ -105,8 +104,8 @@ size_t config_smem(int config, int blob_words, int nk, int R);
 // The autotuned configuration of ks on the current device, else the first one that fits.
 int default_config(const lpaici_kernelset *ks);
 // The adjoint's two passes over storage the caller provides: device copies of ks->blob and ks->adj_blob,
-// D*width*height selection bytes and width*height floats of den.  Allocates nothing.
-int adjoint_passes(const lpaici_kernelset *ks, const int *blob, const int *adj_blob, uint8_t *smap, float *den,
+// D*width*height selection bytes and width*height floats of 1/den.  Allocates nothing.
+int adjoint_passes(const lpaici_kernelset *ks, const int *blob, const int *adj_blob, uint8_t *smap, float *rden,
                    const float *d_noisy, int noisy_pitch, const float *d_grad_out, int gout_pitch, float *d_grad_in,
                    int gin_pitch, int width, int height, float sigma, float gamma, cudaStream_t stream);
 

@@ -284,11 +284,11 @@ __device__ __forceinline__ void sweep_tile(const ImageArgs &img, int x0, int y0,
                 img.out[static_cast<size_t>(oy + 8 * (i & 1)) * img.out_pitch + ox + (i >> 1)] =
                     __fdiv_rn(pick<Q>(num, i), pick<Q>(den, i));
     }
-    if (img.den) {
+    if (img.rden) {
 #pragma unroll
         for (int i = 0; i < 2 * Q; i++)
             if (valid & (1u << i))
-                img.den[static_cast<size_t>(oy + 8 * (i & 1)) * img.W + ox + (i >> 1)] = pick<Q>(den, i);
+                img.rden[static_cast<size_t>(oy + 8 * (i & 1)) * img.W + ox + (i >> 1)] = __frcp_rn(pick<Q>(den, i));
     }
 }
 
