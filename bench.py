@@ -17,10 +17,13 @@ rank's time.
             achieved = 2 x algorithmic taps / kernel time
   cpu_baseline  the reference's own CPU engine (anisotropic_lpa_ici_cpu_fused of
             src/v1_0_lpa_ici_2D_fused.cpp, compiled in-process into oracle/_ref/) on all host cores,
-            one 256x256 crop of the benchmark image per thread
+            one 256x256 crop of the benchmark image per thread; its naive engine (v0_0) beside it
+  parity    the GPU image against those reference outputs, bit for bit, on every crop pixel whose
+            neighbourhood lies inside its crop
   extra     batched persistent forward over 64 images (sides U[256,2048], sigma U[10,40]/255, gamma
             U[1.5,2.5]) in a CUDA graph, and the adjoint on 8 x 1024^2, each against the plain forward
-            on the same images
+            on the same images; forward and adjoint on one 8192^2 image with the gaussian m=(2,0)
+            kernels (sigma 25/255, gamma 1.5); adjoint checked by sum(g*out) = sum(grad*x)
 
 --impl reference runs only the reference's CPU engine (bounded sample per step, all host threads).
 """
@@ -48,6 +51,7 @@ sys.path.insert(0, PKG)
 METRIC = "Mpix/s at 4096^2 16x7: batched+adjoint vs plain on same GPU, max err<=1e-4"
 UNIT = "Mpix/s"
 SYM = "lpa_kernels_m_1_0_d_16_h12_1_2_4_8_16_24_32_symmetric.txt"
+GAUSS_M2 = "lpa_kernels_m_2_0_d_16_h12_1_2_4_8_16_24_32_gaussian.txt"
 SIGMA = float(np.float32(20.0) / np.float32(255.0))
 GAMMA = 2.0
 SEED = 20250910
@@ -164,9 +168,11 @@ def time_launches(torch, fn, steps: int, warmup: int, flush) -> list[float]:
     return ms
 
 
-def cpu_reference_sample(noisy: np.ndarray, crop: int, threads: int, sigma: float, gamma: float, seed: int = 0):
-    """The reference's CPU engine on `threads` distinct crop x crop pieces of `noisy`, one per thread,
-    each denoised as a whole image (as the reference's executables do).  Returns (Mpix/s, seconds)."""
+def cpu_reference_sample(noisy: np.ndarray, crop: int, threads: int, sigma: float, gamma: float, seed: int = 0,
+                         engine: str = "v1_0", keep: bool = False):
+    """The reference's CPU engine (`engine`: v1_0 fused or v0_0 naive) on `threads` distinct crop x crop
+    pieces of `noisy`, one per thread, each denoised as a whole image (as the reference's executables
+    do).  Returns (Mpix/s, seconds, [(y, x, output)] if keep else None)."""
     import concurrent.futures as cf
 
     sys.path.insert(0, os.path.join(ROOT, "tests"))
@@ -174,22 +180,41 @@ def cpu_reference_sample(noisy: np.ndarray, crop: int, threads: int, sigma: floa
 
     H, W = noisy.shape
     rng = np.random.default_rng(seed)
-    crops = []
+    corners, crops = [], []
     for _ in range(threads):
         y, x = (int(v) for v in rng.integers(0, [H - crop + 1, W - crop + 1]))
+        corners.append((y, x))
         crops.append(np.ascontiguousarray(noisy[y:y + crop, x:x + crop]))
     tmp = tempfile.mkdtemp()
     with quiet_stdout():  # the reference prints progress lines on stdout: keep them off the JSON line
         try:
-            k = ob.ref_load_kernels(kernel_path(SYM, tmp))
+            k = ob.ref_load_kernels(kernel_path(SYM, tmp), name=engine)
         finally:
             shutil.rmtree(tmp, ignore_errors=True)
-        var = ob.ref_variances(k, np.float32(sigma))
+        var = ob.ref_variances(k, np.float32(sigma), name=engine)
         t0 = time.perf_counter()
         with cf.ThreadPoolExecutor(max_workers=threads) as ex:
-            list(ex.map(lambda c: ob.ref_forward(c, k, var, gamma), crops))
+            outs = list(ex.map(lambda c: ob.ref_forward(c, k, var, gamma, name=engine), crops))
         secs = time.perf_counter() - t0
-    return threads * crop * crop / secs / 1e6, secs
+    kept = [(y, x, o) for (y, x), o in zip(corners, outs)] if keep else None
+    return threads * crop * crop / secs / 1e6, secs, kept
+
+
+def crop_parity(got: np.ndarray, kept, R: int) -> dict:
+    """The GPU result against the reference's own CPU results on the crops: every crop pixel whose
+    R-neighbourhood lies inside the crop sees the same input as in the full image, so it must match
+    bit for bit."""
+    n = mism = 0
+    err = 0.0
+    for y, x, ref in kept:
+        h, w = ref.shape
+        a = got[y + R:y + h - R, x + R:x + w - R]
+        b = ref[R:h - R, R:w - R]
+        n += a.size
+        mism += int(np.count_nonzero(a.view(np.uint32) != b.view(np.uint32)))
+        err = max(err, float(np.abs(a.astype(np.float64) - b.astype(np.float64)).max()))
+    return {"against": "reference CPU engine (v1_0) on the cpu_baseline crops, interior pixels",
+            "pixels": n, "bit_mismatches": mism, "max_abs_err": err, "bit_exact": mism == 0}
 
 
 class quiet_stdout:
@@ -229,7 +254,7 @@ def run_reference(args, rank: int, world: int) -> None:
         cpu_reference_sample(noisy, 64, threads, SIGMA, GAMMA, seed=1)
     vals, secs = [], []
     for i in range(args.steps):
-        v, s = cpu_reference_sample(noisy, args.ref_crop, threads, SIGMA, GAMMA, seed=100 + i)
+        v, s, _ = cpu_reference_sample(noisy, args.ref_crop, threads, SIGMA, GAMMA, seed=100 + i)
         vals.append(v)
         secs.append(s)
     value = float(np.mean(vals))
@@ -298,8 +323,6 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     px = size * size
     value = world * px / (ms_step * 1e-3) / 1e6
 
-    # parity of this run: two windows against the oracle (window + 31 px halo), bit for bit
-    parity = check_windows(torch, ks, noisy_h, out, rank) if rank == 0 and not args.no_parity else None
 
     # e2e through the C ABI with pinned host buffers
     pin_in = torch.from_numpy(noisy_h).pin_memory()
@@ -330,13 +353,18 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     if rank == 0 and world == 1 and not args.no_extras:
         extra = run_extras(torch, lpaici, ks, args, flush)
 
-    cpu = None
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = host_threads()
-        v, s = cpu_reference_sample(noisy_h, 256, threads, SIGMA, GAMMA)
+        v, s, kept = cpu_reference_sample(noisy_h, 256, threads, SIGMA, GAMMA, keep=True)
+        parity = crop_parity(out.cpu().numpy(), kept, ks.radius)
+        v0, s0, _ = cpu_reference_sample(noisy_h, 128, threads, SIGMA, GAMMA, seed=1, engine="v0_0")
         cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
                "sample": f"{threads} crops of 256x256 px of the benchmark image, one per host thread, each "
-                         f"denoised whole by the reference's anisotropic_lpa_ici_cpu_fused ({s:.1f} s)"}
+                         f"denoised whole by the reference's anisotropic_lpa_ici_cpu_fused ({s:.1f} s)",
+               "v0_0": {"value": v0, "unit": UNIT, "cores": threads,
+                        "sample": f"{threads} crops of 128x128 px, the reference's naive engine "
+                                  f"(src/v0_0_lpa_ici_2D_naive.cpp) ({s0:.1f} s)"}}
 
     if rank != 0:
         if dist:
@@ -376,28 +404,6 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     if dist:
         torch.distributed.barrier()
     shutil.rmtree(tmp, ignore_errors=True)
-
-
-def check_windows(torch, ks, noisy_h, out, rank):
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import oracle_bind as ob
-
-    tmp = tempfile.mkdtemp()
-    try:
-        ko = ob.oracle_load_kernels(kernel_path(SYM, tmp))
-    finally:
-        shutil.rmtree(tmp, ignore_errors=True)
-    var = ks.variances(SIGMA)
-    got = out.cpu().numpy()
-    R, n, ok = ks.radius, 48, True
-    rng = np.random.default_rng(rank)
-    H, W = noisy_h.shape
-    for y, x in [(0, 0)] + [tuple(int(v) for v in rng.integers(0, min(H, W) - n, 2))]:
-        y0, x0, y1, x1 = max(0, y - R), max(0, x - R), min(H, y + n + R), min(W, x + n + R)
-        ref, _, _ = ob.oracle_forward_f32(noisy_h[y0:y1, x0:x1], ko, var, GAMMA)
-        ok &= np.array_equal(got[y:y + n, x:x + n].view(np.uint32),
-                             ref[y - y0:y - y0 + n, x - x0:x - x0 + n].view(np.uint32))
-    return {"windows_vs_oracle": 2, "bit_exact": bool(ok)}
 
 
 def run_extras(torch, lpaici, ks, args, flush) -> dict:
@@ -450,14 +456,54 @@ def run_extras(torch, lpaici, ks, args, flush) -> dict:
 
     a_ms = time_launches(torch, adj, steps, 1, flush)
     f_ms = time_launches(torch, fwd8, steps, 1, flush)
+    ident8 = max(adjoint_identity(torch, x, g, o, gr) for x, g, o, gr in zip(xa, ga, fo, gi))
+    del xa, ga, gi, fo
+    large = run_large(torch, lpaici, steps, flush)
     return {
         "batched": {"images": n, "mpix": total_px / 1e6, "value": total_px / (np.mean(b_ms) * 1e-3) / 1e6,
                     "plain_same_images": total_px / (np.mean(p_ms) * 1e-3) / 1e6, "unit": UNIT,
                     "graph": True, "bit_equal_to_plain": bool(same)},
         "adjoint": {"images": m, "size": 1024, "value": m * 1024 * 1024 / (np.mean(a_ms) * 1e-3) / 1e6,
                     "forward_same_images": m * 1024 * 1024 / (np.mean(f_ms) * 1e-3) / 1e6, "unit": UNIT,
-                    "adjoint_over_forward_time": float(np.mean(a_ms) / np.mean(f_ms))},
+                    "adjoint_over_forward_time": float(np.mean(a_ms) / np.mean(f_ms)),
+                    "identity_rel_err": ident8},
+        "large": large,
     }
+
+
+def adjoint_identity(torch, x, g, out, grad) -> float:
+    """With the selection frozen the forward is linear in its input, out = J x, so
+    sum(g * out) = sum(g * J x) = sum(J^T g * x) = sum(grad * x): the relative gap of the two sums
+    (FP64 reductions of the FP32 results) checks the adjoint at any size."""
+    a = float((g.double() * out.double()).sum())
+    b = float((grad.double() * x.double()).sum())
+    scale = float((g.double().abs() * out.double().abs()).sum())
+    return abs(a - b) / scale
+
+
+def run_large(torch, lpaici, steps, flush) -> dict:
+    """Forward and adjoint (scale maps recomputed in the backward) on one 8192^2 image, gaussian
+    m=(2,0) 16x7 kernels, sigma 25/255, gamma 1.5."""
+    tmp = tempfile.mkdtemp()
+    try:
+        kg = lpaici.KernelSet.load(kernel_path(GAUSS_M2, tmp))
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    n = 8192
+    sigma = float(np.float32(25.0) / np.float32(255.0))
+    gamma = 1.5
+    _, noisy = bench_image(n, SEED, sigma)
+    x = torch.from_numpy(noisy).cuda()
+    g = torch.randn(n, n, generator=torch.Generator().manual_seed(5)).cuda()
+    out = torch.empty_like(x)
+    grad = torch.empty_like(x)
+    f_ms = time_launches(torch, lambda: lpaici.forward(kg, x, sigma, gamma, out=out), steps, 1, flush)
+    a_ms = time_launches(torch, lambda: lpaici.backward(kg, x, g, sigma, gamma, grad_in=grad), steps, 1, flush)
+    ident = adjoint_identity(torch, x, g, out, grad)
+    return {"size": n, "kernels": "gaussian m=(2,0) 16x7", "sigma": sigma, "gamma": gamma,
+            "forward": n * n / (np.mean(f_ms) * 1e-3) / 1e6, "adjoint": n * n / (np.mean(a_ms) * 1e-3) / 1e6,
+            "unit": UNIT, "forward_ms": float(np.mean(f_ms)), "adjoint_ms": float(np.mean(a_ms)),
+            "adjoint_over_forward_time": float(np.mean(a_ms) / np.mean(f_ms)), "identity_rel_err": ident}
 
 
 def run_profile(args) -> None:
@@ -499,7 +545,6 @@ def main():
     ap.add_argument("--ref-crop", type=int, default=256, help="crop side per thread for --impl reference")
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-parity", action="store_true")
     ap.add_argument("--size", type=int, default=SIZE, help="image side (profiling runs use a smaller case)")
     ap.add_argument("--tile-config", type=int, default=-1, help="fixed tile configuration instead of autotuning")
     ap.add_argument("--profile", choices=["forward", "adjoint"], default=None,
