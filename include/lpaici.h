@@ -175,20 +175,24 @@ int lpaici_set_tile_config(lpaici_kernelset *ks, int config);
 /* Gradient of L = sum_p g[p] * denoised[p] with respect to the noisy input, the ICI-selected scales
  * held fixed: grad[q] = sum_d sum_p g[p] * alpha_d(p) * h_{d,s*(d,p)}(q - p + c), with
  * alpha_d(p) = (1/v_d(p)) / sum_d' (1/v_d'(p)).  The selected scales and den are recomputed by an
- * exact forward sweep into a transient workspace (D*width*height bytes + 4*width*height bytes, taken
- * with cudaMallocAsync on `stream` and released stream-ordered); the forward keeps nothing for the
+ * exact forward sweep into a transient workspace (D*width*height bytes + 4*width*height bytes), taken
+ * stream-ordered on `stream` from a memory pool this library owns on each device; the pool keeps freed
+ * memory for later calls (lpaici_trim_workspace returns it).  The forward keeps nothing for the
  * adjoint.  No counterpart in the reference.
  *   d_grad_out  g, width x height (pitch gout_pitch);  d_grad_in  width x height (pitch gin_pitch) */
 int lpaici_backward(const lpaici_kernelset *ks, const float *d_noisy, int noisy_pitch, const float *d_grad_out,
                     int gout_pitch, float *d_grad_in, int gin_pitch, int width, int height, float sigma,
                     float gamma, lpaici_stream_t stream);
 
+/* Returns the memory cached in the adjoint's workspace pool on the current device to the driver. */
+int lpaici_trim_workspace(void);
+
 /* Size of the static device scratch behind lpaici_backward_noalloc: 64 MiB per device. */
 #define LPAICI_NOALLOC_SCRATCH_BYTES (64u << 20)
 
 /* lpaici_backward without any device allocation: same arguments and result (same kernels, so equal to
  * it), with its workspace and both kernel blobs in one file-scope __device__ array of
- * LPAICI_NOALLOC_SCRATCH_BYTES instead of cudaMallocAsync / cudaMalloc.  For callers that cannot
+ * LPAICI_NOALLOC_SCRATCH_BYTES instead of the workspace pool and cudaMalloc.  For callers that cannot
  * allocate device memory during a step: a framework whose caching allocator already holds the free
  * memory, a loop that must not allocate after its setup, a device without stream-ordered memory
  * pools.  No counterpart in the reference.

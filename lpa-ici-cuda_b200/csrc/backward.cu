@@ -16,6 +16,8 @@
 //      deterministic.
 // No counterpart in the reference.
 #include <algorithm>
+#include <cstdint>
+#include <mutex>
 
 #include "configs.h"
 #include "tile_core.cuh"
@@ -282,9 +284,67 @@ int adjoint_passes(const lpaici_kernelset *ks, const int *blob, const int *adj_b
     return e == cudaSuccess ? LPAICI_OK : cuda_error(e, "adjoint gather launch");
 }
 
+namespace {
+
+// The adjoint's workspace comes from a stream-ordered memory pool owned by this library, one per
+// device, that keeps freed memory for the next call (release threshold: never).  The device's default
+// pool returns memory to the driver at every synchronisation, so a caller that synchronises between
+// calls would map the workspace afresh each time (about 20 bytes per pixel: tens of ms at 8192^2).
+constexpr int kMaxPoolDevices = 64;
+std::mutex g_pool_lock;
+cudaMemPool_t g_pools[kMaxPoolDevices];
+
+int workspace_pool(cudaMemPool_t *out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_error(e, "cudaGetDevice");
+    if (dev < 0 || dev >= kMaxPoolDevices)
+        return set_error(LPAICI_ERR_UNSUPPORTED, "device %d beyond %d", dev, kMaxPoolDevices);
+    std::lock_guard<std::mutex> hold(g_pool_lock);
+    if (!g_pools[dev]) {
+        int supported = 0;
+        cudaDeviceGetAttribute(&supported, cudaDevAttrMemoryPoolsSupported, dev);
+        if (!supported)
+            return set_error(LPAICI_ERR_UNSUPPORTED,
+                             "device %d has no stream-ordered memory pools: use lpaici_backward_noalloc", dev);
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        e = cudaMemPoolCreate(&pool, &props);
+        if (e != cudaSuccess) return cuda_error(e, "cudaMemPoolCreate(adjoint workspace)");
+        uint64_t keep = ~uint64_t(0);
+        e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e != cudaSuccess) {
+            cudaMemPoolDestroy(pool);
+            return cuda_error(e, "cudaMemPoolSetAttribute(adjoint workspace)");
+        }
+        g_pools[dev] = pool;
+    }
+    *out = g_pools[dev];
+    return LPAICI_OK;
+}
+
+}  // namespace
+
 }  // namespace lpaici
 
 using namespace lpaici;
+
+extern "C" int lpaici_trim_workspace(void) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_error(e, "cudaGetDevice");
+    cudaMemPool_t pool = nullptr;
+    {
+        std::lock_guard<std::mutex> hold(g_pool_lock);
+        if (dev >= 0 && dev < kMaxPoolDevices) pool = g_pools[dev];
+    }
+    if (!pool) return LPAICI_OK;
+    e = cudaMemPoolTrimTo(pool, 0);
+    return e == cudaSuccess ? LPAICI_OK : cuda_error(e, "cudaMemPoolTrimTo(adjoint workspace)");
+}
 
 extern "C" int lpaici_backward(const lpaici_kernelset *ks, const float *d_noisy, int noisy_pitch,
                                const float *d_grad_out, int gout_pitch, float *d_grad_in, int gin_pitch, int width,
@@ -303,11 +363,14 @@ extern "C" int lpaici_backward(const lpaici_kernelset *ks, const float *d_noisy,
     if (rc != LPAICI_OK) return rc;
 
     // transient workspace: D selection planes (bytes) and 1/den (floats)
+    cudaMemPool_t pool = nullptr;
+    rc = workspace_pool(&pool);
+    if (rc != LPAICI_OK) return rc;
     const size_t npx = static_cast<size_t>(width) * height;
     void *ws = nullptr;
     const size_t smap_bytes = (static_cast<size_t>(ks->D) * npx + 255) & ~size_t(255);
-    cudaError_t e = cudaMallocAsync(&ws, smap_bytes + sizeof(float) * npx, stream);
-    if (e != cudaSuccess) return cuda_error(e, "cudaMallocAsync(adjoint workspace)");
+    cudaError_t e = cudaMallocFromPoolAsync(&ws, smap_bytes + sizeof(float) * npx, pool, stream);
+    if (e != cudaSuccess) return cuda_error(e, "cudaMallocFromPoolAsync(adjoint workspace)");
     uint8_t *smap = static_cast<uint8_t *>(ws);
     float *rden = reinterpret_cast<float *>(static_cast<char *>(ws) + smap_bytes);
     rc = adjoint_passes(ks, blob, adj, smap, rden, d_noisy, noisy_pitch, d_grad_out, gout_pitch, d_grad_in, gin_pitch,

@@ -91,6 +91,7 @@ _SIGS = {
     "lpaici_set_tile_config": ([_vp, _i], _i),
     "lpaici_backward": ([_vp, _vp, _i, _vp, _i, _vp, _i, _i, _i, _f, _f, _vp], _i),
     "lpaici_backward_noalloc": ([_vp, _vp, _i, _vp, _i, _vp, _i, _i, _i, _f, _f, _vp], _i),
+    "lpaici_trim_workspace": ([], _i),
     "lpaici_anisotropic_gpu_fused": ([_fp, _fp, _i, _i, _i, _fp, _i, _i, _fp, _i, _ip, _ip, _ip, _fp, _f,
                                       C.POINTER(C.c_double)], _i),
     "lpaici_denoise_host": ([_vp, _fp, _fp, _i, _i, _f, _f, _vp], _i),
