@@ -56,6 +56,9 @@ SIGMA = float(np.float32(20.0) / np.float32(255.0))
 GAMMA = 2.0
 SEED = 20250910
 SIZE = 4096
+# DRAM bytes of one forward launch on the 4096^2 workload, read + written, from an ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum): the halo re-reads are served by L2.
+FORWARD_DRAM_BYTES = 95.4e6
 
 
 def kernel_path(name: str, tmp: str) -> str:
@@ -385,7 +388,10 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
                    "tile": {"config": best, "tile_w": tw, "tile_h": th, "threads": thr, "pixels_per_thread": ppt},
                    "parallelism": f"dp{world} (independent images, no collective)"},
         "roofline": {"bound": "fp32", "achieved": achieved / 1e12, "peak": peak_ops / 1e12, "unit": "TFLOP/s",
-                     "frac": achieved / peak_ops, "traffic": None,
+                     "frac": achieved / peak_ops, "traffic": FORWARD_DRAM_BYTES if size == SIZE else None,
+                     "traffic_note": "bytes per launch, dram__bytes_read.sum + dram__bytes_write.sum of one ncu "
+                                     "capture of this workload (67.3 MB read + 28.1 MB written; algorithmic "
+                                     "134.2 MB: 4 B in + 4 B out per pixel)",
                      "note": "FLOP = 2 per algorithmic tap (multiply and add, each rounded: bit-exact with the "
                              "reference); peak = the faster of the two exact FP32 forms measured live on this GPU "
                              "(scalar FMUL+FADD, packed fma(w,x,-0)+add); scalar FFMA shown for context",

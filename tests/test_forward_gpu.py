@@ -183,3 +183,26 @@ def test_invalid_arguments(torch):
                               None) == lpaici.ERR_INVALID_ARG
     assert lib.lpaici_forward(None, x.data_ptr(), 8, x.data_ptr(), 8, 8, 8, 0.1, 2.0, None,
                               None) == lpaici.ERR_INVALID_ARG
+
+
+def test_error_against_fp64():
+    """The error of the FP32 result (the reference's own arithmetic, reproduced bit for bit) against the
+    FP64 oracle on the 512^2 baseline image: selected scales agree on >= 99.99 % of (direction, pixel)
+    -- they differ only where an interval test ties within FP32 rounding --, pixels whose 16 scales all
+    agree are within 2e-6 of FP64, PSNR within 0.01 dB.  Measured: 7 of 262,144 pixels carry a
+    flipped scale (max err 2.7e-3 there), 5.1e-7 elsewhere."""
+    import torch
+
+    ks = lpaici.KernelSet.load(kernel_file(SYM))
+    ko = ob.oracle_load_kernels(kernel_file(SYM))
+    clean = lpaici.synth_image(512, 512, 20250910)
+    noisy = lpaici.add_noise(clean, SIGMA_20, 20250910)
+    out, smap = lpaici.forward(ks, torch.from_numpy(noisy).cuda(), SIGMA_20, 2.0, scale_map=True)
+    out, smap = out.cpu().numpy(), smap.cpu().numpy()
+    o64, m64 = ob.oracle_forward_f64(noisy, ko, SIGMA_20, 2.0, want_map=True)
+    assert (smap == m64).mean() >= 0.9999
+    same = (smap == m64).all(axis=0)
+    assert same.mean() >= 0.999
+    assert np.abs(out.astype(np.float64) - o64)[same].max() <= 2e-6
+    psnr64 = 10.0 * np.log10(1.0 / np.mean((clean.astype(np.float64) - o64) ** 2))
+    assert abs(lpaici.psnr(clean, out) - psnr64) <= 0.01
