@@ -160,6 +160,9 @@ int lpaici_batch_create(const lpaici_kernelset *ks, const lpaici_image *images, 
     *out = nullptr;
     cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
     const int nk = ks->D * ks->S;
+    if (ks->S > kMaxScales)
+        return set_error(LPAICI_ERR_UNSUPPORTED, "%d scales per direction; the kernels support at most %d", ks->S,
+                         kMaxScales);
     for (int i = 0; i < n; i++) {
         const lpaici_image &im = images[i];
         if (!im.noisy || !im.denoised || im.width <= 0 || im.height <= 0 || im.noisy_pitch < im.width ||

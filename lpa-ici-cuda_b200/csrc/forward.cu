@@ -77,6 +77,9 @@ size_t config_smem(int config, int blob_words, int nk, int R) {
 int launch_forward(const lpaici_kernelset *ks, const ImageArgs &img, const KernelTables &tab, int config,
                    cudaStream_t stream) {
     (void)ks;
+    if (tab.S > kMaxScales)
+        return set_error(LPAICI_ERR_UNSUPPORTED, "%d scales per direction; the kernels support at most %d", tab.S,
+                         kMaxScales);
     switch (config) {
         LPAICI_TILE_CONFIGS(LPAICI_FWD_CASE)
         default: return set_error(LPAICI_ERR_INVALID_ARG, "tile config %d out of range", config);

@@ -16,6 +16,8 @@ namespace lpaici {
 // parameters (2 * 4 B * kMaxKernels), so D*S is capped; the radius bounds the shared-memory halo.
 constexpr int kMaxKernels = 256;
 constexpr int kMaxRadius = 127;
+// The sweeps keep each pixel's selected scale in 4 bits.
+constexpr int kMaxScales = 16;
 
 // One row run of a kernel, as the device reads it: the taps (dy, dx0 + j), j < len, whose weights
 // are wdup[wofs + j] = {w_j, w_j}.  dy/dx0 are offsets from the output pixel

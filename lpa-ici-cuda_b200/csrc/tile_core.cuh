@@ -24,6 +24,8 @@
 //   num  += est * (1/var); den += 1/var (in direction order, 1/var correctly rounded);  out = num / den.
 #pragma once
 
+#include <type_traits>
+
 #include "internal.h"
 
 namespace lpaici {
@@ -185,25 +187,32 @@ struct LaneGeom {
 template <int Q>
 __device__ __forceinline__ float pick(const float2 (&v)[Q], int i) { return (i & 1) ? v[i >> 1].y : v[i >> 1].x; }
 
-// The ICI scale sweep of direction d for the thread's 2Q pixels (mask `valid`): estimate and index of
-// the last accepted scale of every pixel (sidx: 4 bits per pixel).  Warp-uniform scale loop; it ends
-// when every pixel of the warp has stopped.
+// Per-thread selected-scale indices, 4 bits per pixel.
+template <int Q>
+using ScaleBits = typename std::conditional<(8 * Q <= 32), unsigned, unsigned long long>::type;
+
+// The ICI scale sweep of direction d for the thread's 2Q pixels (mask `valid`): per pixel the estimate
+// of the last accepted scale (best) and that scale's index (sidx, 4 bits per pixel).  The intersection
+// [lo, hi] only shrinks, so once it is empty no later scale can be accepted: a stopped pixel needs no
+// mask, its updates simply never accept again.  Scale 0 is always accepted (lo = -inf, hi = +inf), so
+// the index is the count of accepted scales after it.  Warp-uniform scale loop; it ends when every
+// valid pixel of the warp has stopped.
 template <int Q>
 __device__ __forceinline__ void direction_sweep(int d, int S, unsigned valid, const float2 *lane_tile, int pitch2,
                                                 const int *s_blob, const int4 *s_runs, const float4 *s_wq,
-                                                const float *s_thr, float2 nz, float (&best)[2 * Q],
-                                                unsigned long long &sidx) {
+                                                const float *s_thr, float2 nz, float2 (&best)[Q], ScaleBits<Q> &sidx) {
     float lo[2 * Q], hi[2 * Q];
 #pragma unroll
     for (int i = 0; i < 2 * Q; i++) {
         lo[i] = -INFINITY;
         hi[i] = INFINITY;
-        best[i] = 0.0f;
     }
+#pragma unroll
+    for (int m = 0; m < Q; m++) best[m] = make_float2(0.0f, 0.0f);
     sidx = 0;
-    unsigned alive = valid;
+    bool alive = valid != 0;
     for (int s = 0; s < S; s++) {
-        if (!__any_sync(0xffffffffu, alive)) break;  // every pixel of the warp has stopped
+        if (!__any_sync(0xffffffffu, alive)) break;  // every valid pixel of the warp has stopped
         const int k = d * S + s;
         float2 acc[Q];
 #pragma unroll
@@ -214,24 +223,25 @@ __device__ __forceinline__ void direction_sweep(int d, int S, unsigned valid, co
             conv_run<Q>(acc, lane_tile + run.x * pitch2 + run.y, s_wq + (run.w >> 1), run.z, nz);
         }
         const float thr = s_thr[k];
+        const ScaleBits<Q> step = s > 0 ? 1 : 0;
         float2 lb[Q], ub[Q];
 #pragma unroll
         for (int m = 0; m < Q; m++) {
             lb[m] = add2(acc[m], make_float2(-thr, -thr));  // conv - thr, exactly
             ub[m] = add2(acc[m], make_float2(thr, thr));
         }
+        alive = false;
 #pragma unroll
         for (int i = 0; i < 2 * Q; i++) {
-            if (alive & (1u << i)) {
-                lo[i] = fmaxf(lo[i], pick<Q>(lb, i));
-                hi[i] = fminf(hi[i], pick<Q>(ub, i));
-                if (hi[i] >= lo[i]) {
-                    best[i] = pick<Q>(acc, i);
-                    sidx = (sidx & ~(15ull << (4 * i))) | (static_cast<unsigned long long>(s) << (4 * i));
-                } else {
-                    alive &= ~(1u << i);
-                }
-            }
+            lo[i] = fmaxf(lo[i], pick<Q>(lb, i));
+            hi[i] = fminf(hi[i], pick<Q>(ub, i));
+            const bool ok = hi[i] >= lo[i];
+            if (i & 1)
+                best[i >> 1].y = ok ? acc[i >> 1].y : best[i >> 1].y;
+            else
+                best[i >> 1].x = ok ? acc[i >> 1].x : best[i >> 1].x;
+            sidx += ok ? static_cast<ScaleBits<Q>>(step << (4 * i)) : ScaleBits<Q>(0);
+            alive |= ok && ((valid >> i) & 1u);
         }
     }
 }
@@ -259,14 +269,14 @@ __device__ __forceinline__ void sweep_tile(const ImageArgs &img, int x0, int y0,
     for (int m = 0; m < Q; m++) num[m] = den[m] = make_float2(0.0f, 0.0f);
 
     for (int d = 0; d < D; d++) {
-        float best[2 * Q];
-        unsigned long long sidx;
+        float2 best[Q];
+        ScaleBits<Q> sidx;
         direction_sweep<Q>(d, S, valid, lane_tile, g.pitch2, s_blob, s_runs, s_wq, s_thr, nz, best, sidx);
 #pragma unroll
         for (int m = 0; m < Q; m++) {
             const float2 r = make_float2(s_rvar[d * S + static_cast<int>((sidx >> (8 * m)) & 15)],
                                          s_rvar[d * S + static_cast<int>((sidx >> (8 * m + 4)) & 15)]);
-            num[m] = add2(num[m], prod2(make_float2(best[2 * m], best[2 * m + 1]), r, nz));
+            num[m] = add2(num[m], prod2(best[m], r, nz));
             den[m] = add2(den[m], r);
         }
         if (img.smap) {
