@@ -100,7 +100,20 @@ class Clocks:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
+
+    def wait_samples(self, n: int, keep_busy, timeout_s: float = 5.0) -> None:
+        """Runs keep_busy() (untimed GPU work) until the sampler has delivered n lines, so the
+        timed region starts with the sampler already running under load."""
+        t_end = time.perf_counter() + timeout_s
+        while self.proc is not None and len(self.lines) < n and time.perf_counter() < t_end:
+            keep_busy()
+
+    def mark(self, start: bool) -> None:
+        if start:
+            self.t0 = time.perf_counter()
+        else:
+            self.t1 = time.perf_counter()
 
     def stop(self) -> dict:
         if self.proc is None:
@@ -113,7 +126,12 @@ class Clocks:
         self.thread.join(timeout=2)
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        # samples taken while the timed steps ran; nvidia-smi delivers one every ~10-100 ms, so a short
+        # region is widened by 150 ms on each side, where the GPU runs the warm-up steps and the flush
+        t0, t1 = getattr(self, "t0", 0.0) - 0.15, getattr(self, "t1", float("inf")) + 0.15
+        for t, ln in self.lines:
+            if not t0 <= t <= t1:
+                continue
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 8:
                 continue
@@ -128,7 +146,7 @@ class Clocks:
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "window": "timed region +- 150 ms"}
 
 
 def fp32_peak() -> dict:
@@ -303,18 +321,19 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     del smap
 
     fwd = lambda: lpaici.forward(ks, x, SIGMA, GAMMA, out=out)  # noqa: E731
+    clocks = Clocks(local_rank)
+    clocks.start()
     for _ in range(args.warmup):
         fwd()
     torch.cuda.synchronize()
+    clocks.wait_samples(2, lambda: (fwd(), torch.cuda.synchronize()))  # more untimed warm-up steps
     if dist:
         torch.distributed.barrier()
-    clocks = Clocks(local_rank)
-    clocks.start()
     torch.cuda.synchronize()
-    if dist:
-        torch.distributed.barrier()
+    clocks.mark(True)
     ms = time_launches(torch, fwd, args.steps, 0, flush)
     torch.cuda.synchronize()
+    clocks.mark(False)
     if dist:
         torch.distributed.barrier()
     clk = clocks.stop()
