@@ -75,6 +75,13 @@ int lpaici_kernelset_load(const char *path, lpaici_kernelset **out);
 int lpaici_kernelset_create(const float *weights, const int *offsets, const int *rows, const int *cols,
                             int num_dirs, int num_scales, lpaici_kernelset **out);
 
+/* Writes the kernel set as a binary tap-list file: the kernel sizes and the run-length packing (the
+ * packer's runs and weights, little-endian, FNV-1a checked).  lpaici_kernelset_load reads such a file
+ * as well as the text format (it tells them apart by the file's first 8 bytes, "LPAICIT1"), and the
+ * command line's -k accepts it: the loader skips the text parse and rebuilds the same kernel set
+ * (dense values outside the runs come back as +0).  No counterpart in the reference. */
+int lpaici_kernelset_save(const lpaici_kernelset *ks, const char *path);
+
 int lpaici_kernelset_destroy(lpaici_kernelset *ks);
 
 int lpaici_kernelset_get_info(const lpaici_kernelset *ks, lpaici_kernelset_info_t *info);

@@ -39,7 +39,7 @@ void usage(const char *prog) {
     const Config d;
     std::cout << "Usage: " << prog << " [options]\n"
               << "  -i, --image <file>     input image (default " << d.image_file << ")\n"
-              << "  -k, --kernels <file>   LPA kernel file (default " << d.kernel_file << ")\n"
+              << "  -k, --kernels <file>   LPA kernel file, text or binary tap-list (default " << d.kernel_file << ")\n"
               << "  -o, --output <file>    denoised .hdr output (default <image dir>/<image name>_<version>.hdr)\n"
               << "  -s, --sigma <value>    noise standard deviation on the 0-255 scale (default 20)\n"
               << "  -g, --gamma <value>    ICI threshold (default " << d.ici_gamma << ")\n"

@@ -262,6 +262,90 @@ struct Stream {
 
 using namespace lpaici;
 
+// ---------------------------------------------------------------------------------------------
+// Binary tap-list file (lpaici_kernelset_save): the run-length packing of every kernel, which
+// together with the kernel sizes restores the loader's cropped dense output (zero outside the runs).
+//   "LPAICIT1"  int32 D, S  int32 rows[nk], cols[nk]  int32 n_runs, n_taps  int32 first_run[nk+1]
+//   int32 dy[n_runs], dx0[n_runs], len[n_runs]  float w[n_taps]  uint64 FNV-1a of all bytes before
+// Little-endian; offsets dy, dx0 are centre-relative as in build_sparse_kernels.
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+constexpr char kTapMagic[8] = {'L', 'P', 'A', 'I', 'C', 'I', 'T', '1'};
+
+uint64_t fnv1a(const char *p, size_t n) {
+    uint64_t h = 1469598103934665603ull;
+    for (size_t i = 0; i < n; i++) {
+        h ^= static_cast<unsigned char>(p[i]);
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+struct Reader {
+    const char *p, *end;
+    template <typename T>
+    bool get(T *dst, size_t n) {
+        const size_t bytes = sizeof(T) * n;
+        if (static_cast<size_t>(end - p) < bytes) return false;
+        std::memcpy(dst, p, bytes);
+        p += bytes;
+        return true;
+    }
+};
+
+// Fills ks (D, S, dense arrays) from a tap-list file image; LPAICI_OK or LPAICI_ERR_KERNEL_FORMAT.
+int parse_tap_file(const std::string &bytes, const char *path, lpaici_kernelset *ks) {
+    const size_t body = bytes.size() >= sizeof(uint64_t) ? bytes.size() - sizeof(uint64_t) : 0;
+    uint64_t stored = 0;
+    if (body < sizeof(kTapMagic)) return set_error(LPAICI_ERR_KERNEL_FORMAT, "%s: truncated tap-list file", path);
+    std::memcpy(&stored, bytes.data() + body, sizeof(stored));
+    if (stored != fnv1a(bytes.data(), body))
+        return set_error(LPAICI_ERR_KERNEL_FORMAT, "%s: tap-list checksum mismatch", path);
+    Reader rd{bytes.data() + sizeof(kTapMagic), bytes.data() + body};
+    int D = 0, S = 0;
+    if (!rd.get(&D, 1) || !rd.get(&S, 1) || D <= 0 || S <= 0)
+        return set_error(LPAICI_ERR_KERNEL_FORMAT, "%s: bad tap-list header", path);
+    if (static_cast<long>(D) * S > kMaxKernels)
+        return set_error(LPAICI_ERR_UNSUPPORTED, "%s has %d x %d kernels; at most %d", path, D, S, kMaxKernels);
+    const int nk = D * S;
+    std::vector<int> rows(nk), cols(nk), first(nk + 1);
+    int n_runs = 0, n_taps = 0;
+    if (!rd.get(rows.data(), nk) || !rd.get(cols.data(), nk) || !rd.get(&n_runs, 1) || !rd.get(&n_taps, 1) ||
+        n_runs < 0 || n_taps < 0 || n_runs > (1 << 26) || n_taps > (1 << 28) || !rd.get(first.data(), nk + 1))
+        return set_error(LPAICI_ERR_KERNEL_FORMAT, "%s: truncated tap-list file", path);
+    std::vector<int> dy(n_runs), dx0(n_runs), len(n_runs);
+    std::vector<float> w(n_taps);
+    if (!rd.get(dy.data(), n_runs) || !rd.get(dx0.data(), n_runs) || !rd.get(len.data(), n_runs) ||
+        !rd.get(w.data(), n_taps) || rd.p != rd.end)
+        return set_error(LPAICI_ERR_KERNEL_FORMAT, "%s: tap-list sizes do not match the file", path);
+    if (first[0] != 0 || first[nk] != n_runs)
+        return set_error(LPAICI_ERR_KERNEL_FORMAT, "%s: bad run ranges", path);
+    ks->D = D;
+    ks->S = S;
+    long taps = 0;
+    for (int k = 0; k < nk; k++) {
+        if (rows[k] <= 0 || cols[k] <= 0 || static_cast<long>(rows[k]) * cols[k] > (1L << 26) || first[k + 1] < first[k])
+            return set_error(LPAICI_ERR_KERNEL_FORMAT, "%s: bad size or run range of kernel %d", path, k);
+        ks->off.push_back(static_cast<int>(ks->dense_w.size()));
+        ks->rows.push_back(rows[k]);
+        ks->cols.push_back(cols[k]);
+        const size_t base = ks->dense_w.size();
+        ks->dense_w.resize(base + static_cast<size_t>(rows[k]) * cols[k], 0.0f);
+        for (int r = first[k]; r < first[k + 1]; r++) {
+            const int row = dy[r] + rows[k] / 2, col = dx0[r] + cols[k] / 2;
+            if (row < 0 || row >= rows[k] || col < 0 || len[r] <= 0 || col + len[r] > cols[k] || taps + len[r] > n_taps)
+                return set_error(LPAICI_ERR_KERNEL_FORMAT, "%s: run %d lies outside kernel %d", path, r, k);
+            std::memcpy(&ks->dense_w[base + static_cast<size_t>(row) * cols[k] + col], &w[taps], sizeof(float) * len[r]);
+            taps += len[r];
+        }
+    }
+    if (taps != n_taps) return set_error(LPAICI_ERR_KERNEL_FORMAT, "%s: %ld taps in runs, %d stored", path, taps, n_taps);
+    return LPAICI_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 const char *lpaici_last_error(void) { return g_last_error.c_str(); }
@@ -287,6 +371,26 @@ int lpaici_kernelset_load(const char *path, lpaici_kernelset **out) {
     std::stringstream ss;
     ss << f.rdbuf();
     const std::string text = ss.str();
+    if (text.size() >= sizeof(kTapMagic) && std::memcmp(text.data(), kTapMagic, sizeof(kTapMagic)) == 0) {
+        auto *ks = new lpaici_kernelset();
+        int rc = parse_tap_file(text, path, ks);
+        if (rc == LPAICI_OK) rc = finish_kernelset(ks);
+        if (rc == LPAICI_OK) {
+            int ndev = 0;
+            if (cudaGetDeviceCount(&ndev) == cudaSuccess && ndev > 0) {
+                const int *p = nullptr;
+                rc = device_blob(ks, &p);
+            } else {
+                cudaGetLastError();
+            }
+        }
+        if (rc != LPAICI_OK) {
+            delete ks;
+            return rc;
+        }
+        *out = ks;
+        return LPAICI_OK;
+    }
     Stream tk{text.data(), text.data() + text.size()};
 
     int D = 0, S = 0;
@@ -391,6 +495,35 @@ int lpaici_kernelset_create(const float *weights, const int *offsets, const int 
         cudaGetLastError();
     }
     *out = ks;
+    return LPAICI_OK;
+}
+
+int lpaici_kernelset_save(const lpaici_kernelset *ks, const char *path) {
+    if (!ks || !path) return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_kernelset_save: null argument");
+    const int nk = ks->D * ks->S;
+    std::string b(kTapMagic, sizeof(kTapMagic));
+    auto put = [&b](const void *p, size_t n) { b.append(static_cast<const char *>(p), n); };
+    const int n_runs = static_cast<int>(ks->run_row.size()), n_taps = static_cast<int>(ks->run_w.size());
+    std::vector<int> first(ks->k_first_run);
+    first.push_back(n_runs);
+    put(&ks->D, sizeof(int));
+    put(&ks->S, sizeof(int));
+    put(ks->rows.data(), sizeof(int) * nk);
+    put(ks->cols.data(), sizeof(int) * nk);
+    put(&n_runs, sizeof(int));
+    put(&n_taps, sizeof(int));
+    put(first.data(), sizeof(int) * (nk + 1));
+    put(ks->run_row.data(), sizeof(int) * n_runs);
+    put(ks->run_col.data(), sizeof(int) * n_runs);
+    put(ks->run_len.data(), sizeof(int) * n_runs);
+    put(ks->run_w.data(), sizeof(float) * n_taps);
+    const uint64_t h = fnv1a(b.data(), b.size());
+    put(&h, sizeof(h));
+    std::ofstream f(path, std::ios::binary | std::ios::trunc);
+    if (!f.is_open()) return set_error(LPAICI_ERR_FILE, "cannot create %s", path);
+    f.write(b.data(), static_cast<std::streamsize>(b.size()));
+    f.close();
+    if (!f) return set_error(LPAICI_ERR_FILE, "cannot write %s", path);
     return LPAICI_OK;
 }
 

@@ -73,6 +73,7 @@ _SIGS = {
     "lpaici_status_string": ([_i], C.c_char_p),
     "lpaici_kernelset_load": ([C.c_char_p, C.POINTER(_vp)], _i),
     "lpaici_kernelset_create": ([_fp, _ip, _ip, _ip, _i, _i, C.POINTER(_vp)], _i),
+    "lpaici_kernelset_save": ([_vp, C.c_char_p], _i),
     "lpaici_kernelset_destroy": ([_vp], _i),
     "lpaici_kernelset_get_info": ([_vp, C.POINTER(KernelSetInfo)], _i),
     "lpaici_kernelset_get_dense": ([_vp, _fp, _ip, _ip, _ip], _i),
@@ -160,6 +161,10 @@ class KernelSet:
         _check(_lib.lpaici_kernelset_create(_fptr(w), _iptr(o), _iptr(r), _iptr(c), num_dirs, num_scales,
                                             C.byref(h)), "lpaici_kernelset_create")
         return cls(h.value)
+
+    def save(self, path: str) -> None:
+        """Writes the binary tap-list file that load() reads back (lpaici_kernelset_save)."""
+        _check(_lib.lpaici_kernelset_save(self.handle, os.fsencode(path)), f"lpaici_kernelset_save({path})")
 
     def close(self) -> None:
         if self._h and self._h.value:
