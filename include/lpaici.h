@@ -191,6 +191,31 @@ int lpaici_backward(const lpaici_kernelset *ks, const float *d_noisy, int noisy_
                     int gout_pitch, float *d_grad_in, int gin_pitch, int width, int height, float sigma,
                     float gamma, lpaici_stream_t stream);
 
+/* One image of a batched adjoint: noisy input, cotangent g and the gradient's buffer (device pointers,
+ * pitches in floats), with the image's sigma and gamma. */
+typedef struct {
+    const float *noisy;
+    const float *grad_out;
+    float *grad_in;
+    int width, height;
+    int noisy_pitch, gout_pitch, gin_pitch;
+    float sigma, gamma;
+} lpaici_grad_image;
+
+typedef struct lpaici_backward_batch lpaici_backward_batch;
+
+/* Plans the adjoint of many images: pass A (selection) as one persistent launch over all images'
+ * tiles (the forward batch kernel writing s* and 1/den into memory the plan owns, D+4 bytes per
+ * pixel), pass B (gather) as one launch over all images' tiles; with use_graph both are captured in
+ * one CUDA graph.  Gradients equal lpaici_backward's, image by image, bit for bit.  The pointers are
+ * baked in: rerun when the contents change, re-plan when the pointers change.  No counterpart in the
+ * reference. */
+int lpaici_backward_batch_create(const lpaici_kernelset *ks, const lpaici_grad_image *images, int n,
+                                 const lpaici_batch_options *opts, lpaici_stream_t stream,
+                                 lpaici_backward_batch **out);
+int lpaici_backward_batch_run(lpaici_backward_batch *b, lpaici_stream_t stream);
+int lpaici_backward_batch_destroy(lpaici_backward_batch *b);
+
 /* Returns the memory cached in the adjoint's workspace pool on the current device to the driver. */
 int lpaici_trim_workspace(void);
 

@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <mutex>
+#include <vector>
 
 #include "configs.h"
 #include "tile_core.cuh"
@@ -35,17 +36,26 @@ constexpr int kGatherGroups = 2;
 constexpr int kGroupThreads = 32 * kGatherWX * kGatherWY;
 constexpr int kGatherThreads = kGatherGroups * kGroupThreads;
 
-struct GatherArgs {
+// One image of the gather: pass A's outputs and the caller's buffers.
+struct GatherImage {
     const float *g;        // cotangent, pitch g_pitch
     const uint8_t *smap;   // D x H x W selected scales (pass A)
     const float *rden;     // H x W, pitch W: 1 / den, den = sum_d 1/v_d (pass A)
     float *grad;           // result, pitch grad_pitch
+    const float *rvar;     // 1 / v_k of this image (batched plans; one image: GatherArgs::rvar)
     int g_pitch, grad_pitch, W, H;
+    int tiles_x, pad;
+};
+
+struct GatherArgs {
+    GatherImage single;          // the image of a one-image launch (images == null)
+    const GatherImage *images;   // batched: per-image descriptors in device memory
+    const int2 *items;           // batched: (image, tile) of every CTA
     int D, S, R;
     const int *blob;       // mirrored kernels (lpaici_kernelset::adj_blob)
     int blob_words, run_word, weight_word;
     int pitch, rows;       // shared-memory field geometry (floats)
-    float rvar[kMaxKernels];  // 1 / v_k
+    float rvar[kMaxKernels];  // 1 / v_k of the one image
     // per kernel: the field rectangle its gathers read, rows [x, y), 4-column groups [z, w)
     int4 rect[kMaxKernels];
 };
@@ -95,7 +105,17 @@ __global__ void __launch_bounds__(kGatherThreads, 1) lpaici_adjoint_gather_kerne
     float *s_u = reinterpret_cast<float *>(smem + a.blob_words);  // u = g / den on the halo'd tile
     float *s_f = s_u + fsize;                                     // the masked field of one kernel
     uint8_t *s_s = reinterpret_cast<uint8_t *>(s_f + fsize);      // s*(d, .) on the halo'd tile
-    const int x0 = blockIdx.x * kGatherTW, y0 = blockIdx.y * kGatherTH;
+    GatherImage im;
+    int tile = blockIdx.x;
+    if (a.images) {
+        const int2 it = a.items[blockIdx.x];
+        im = a.images[it.x];
+        tile = it.y;
+    } else {
+        im = a.single;
+    }
+    const float *rvar_k = a.images ? im.rvar : a.rvar;
+    const int x0 = (tile % im.tiles_x) * kGatherTW, y0 = (tile / im.tiles_x) * kGatherTH;
     const int gx0 = x0 - a.R, gy0 = y0 - a.R;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = kGatherThreads >> 5;
     const int group = threadIdx.x / kGroupThreads, gtid = threadIdx.x % kGroupThreads, gwarp = gtid >> 5;
@@ -110,19 +130,19 @@ __global__ void __launch_bounds__(kGatherThreads, 1) lpaici_adjoint_gather_kerne
     stage_words(s_blob, a.blob, a.blob_words);
     for (int r = warp; r < a.rows; r += nwarps) {  // one warp per row, lanes along it
         const int gy = gy0 + r;
-        const bool row_ok = gy >= 0 && gy < a.H;
+        const bool row_ok = gy >= 0 && gy < im.H;
         for (int cc = lane; cc < a.pitch; cc += 32) {
             const int gx = gx0 + cc;
             float u = 0.0f;
-            if (row_ok && gx >= 0 && gx < a.W)
-                u = a.g[static_cast<size_t>(gy) * a.g_pitch + gx] * a.rden[static_cast<size_t>(gy) * a.W + gx];
+            if (row_ok && gx >= 0 && gx < im.W)
+                u = im.g[static_cast<size_t>(gy) * im.g_pitch + gx] * im.rden[static_cast<size_t>(gy) * im.W + gx];
             s_u[r * a.pitch + cc] = u;
         }
     }
     __syncthreads();
     // alpha's 1/v_k moves into kernel k's weights: sum_t (w_t / v_k) u(p_t)
     for (int k = threadIdx.x; k < nk; k += kGatherThreads) {
-        const float rv = a.rvar[k];
+        const float rv = rvar_k[k];
         for (int r = s_blob[k]; r < s_blob[k + 1]; r++) {
             const int4 run = s_runs[r];
             for (int j = 0; j < run.z; j++) s_w[run.w + j] *= rv;
@@ -138,15 +158,15 @@ __global__ void __launch_bounds__(kGatherThreads, 1) lpaici_adjoint_gather_kerne
         if (threadIdx.x == 0) s_present = 0u;
         __syncthreads();
         unsigned present = 0;
-        const uint8_t *plane = a.smap + static_cast<size_t>(d) * a.H * a.W;
+        const uint8_t *plane = im.smap + static_cast<size_t>(d) * im.H * im.W;
         for (int r = warp; r < a.rows; r += nwarps) {
             const int gy = gy0 + r;
-            const bool row_ok = gy >= 0 && gy < a.H;
+            const bool row_ok = gy >= 0 && gy < im.H;
             for (int cc = lane; cc < a.pitch; cc += 32) {
                 const int gx = gx0 + cc;
                 uint8_t s = 0xff;
-                if (row_ok && gx >= 0 && gx < a.W) {
-                    s = plane[static_cast<size_t>(gy) * a.W + gx];
+                if (row_ok && gx >= 0 && gx < im.W) {
+                    s = plane[static_cast<size_t>(gy) * im.W + gx];
                     present |= 1u << s;
                 }
                 s_s[r * a.pitch + cc] = s;
@@ -187,71 +207,40 @@ __global__ void __launch_bounds__(kGatherThreads, 1) lpaici_adjoint_gather_kerne
     }
     __syncthreads();
     const int oy = y0 + ty;
-    if (group == 0 && oy < a.H) {
-        float *o = a.grad + static_cast<size_t>(oy) * a.grad_pitch + x0 + tx;
+    if (group == 0 && oy < im.H) {
+        float *o = im.grad + static_cast<size_t>(oy) * im.grad_pitch + x0 + tx;
 #pragma unroll
         for (int i = 0; i < P; i++)
-            if (x0 + tx + i < a.W) o[i] = acc[i] + s_f[i * kGroupThreads + gtid];
+            if (x0 + tx + i < im.W) o[i] = acc[i] + s_f[i * kGroupThreads + gtid];
     }
 }
 
 }  // namespace
 
-// The two passes over caller-provided storage (lpaici_backward, lpaici_backward_noalloc).
-int adjoint_passes(const lpaici_kernelset *ks, const int *blob, const int *adj_blob, uint8_t *smap, float *rden,
-                   const float *d_noisy, int noisy_pitch, const float *d_grad_out, int gout_pitch, float *d_grad_in,
-                   int gin_pitch, int width, int height, float sigma, float gamma, cudaStream_t stream) {
-    GatherArgs ga{};
-    ga.R = ks->radius;
-    ga.pitch = field_pitch(kGatherTW + 2 * ga.R + kGatherP);
-    ga.rows = kGatherTH + 2 * ga.R;
-    ga.blob_words = static_cast<int>(ks->adj_blob.size());
-    const size_t fsize = static_cast<size_t>(ga.pitch) * ga.rows;
-    const size_t smem = sizeof(int) * ga.blob_words + 2 * sizeof(float) * fsize + fsize;
+namespace {
+
+// The launch-independent part of the gather's arguments: field geometry, mirrored kernels and the
+// per-kernel rectangles; smem receives the dynamic shared memory, checked against the device.
+int gather_setup(const lpaici_kernelset *ks, const int *adj_blob, GatherArgs *ga, size_t *smem) {
+    ga->R = ks->radius;
+    ga->pitch = field_pitch(kGatherTW + 2 * ga->R + kGatherP);
+    ga->rows = kGatherTH + 2 * ga->R;
+    ga->blob_words = static_cast<int>(ks->adj_blob.size());
+    const size_t fsize = static_cast<size_t>(ga->pitch) * ga->rows;
+    *smem = sizeof(int) * ga->blob_words + 2 * sizeof(float) * fsize + fsize;
     int dev = 0, max_optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    if (smem > static_cast<size_t>(max_optin))
-        return set_error(LPAICI_ERR_UNSUPPORTED, "adjoint tile needs %zu B of shared memory, device allows %d", smem,
+    if (*smem > static_cast<size_t>(max_optin))
+        return set_error(LPAICI_ERR_UNSUPPORTED, "adjoint tile needs %zu B of shared memory, device allows %d", *smem,
                          max_optin);
-    const dim3 grid((width + kGatherTW - 1) / kGatherTW, (height + kGatherTH - 1) / kGatherTH);
-    if (grid.y > 65535u) return set_error(LPAICI_ERR_UNSUPPORTED, "image too tall: %d rows", height);
-
-    // A. selection
-    ImageArgs img{};
-    img.in = d_noisy;
-    img.out = nullptr;
-    img.smap = smap;
-    img.rden = rden;
-    img.W = width;
-    img.in_h = height;
-    img.in_pitch = noisy_pitch;
-    img.out_pitch = width;
-    img.row_begin = 0;
-    img.rows_out = height;
-    KernelTables tab;
-    fill_tables(ks, nullptr, sigma, gamma, &tab);
-    tab.blob = blob;
-    int rc = launch_forward(ks, img, tab, default_config(ks), stream);
-    if (rc != LPAICI_OK) return rc;
-
-    // B. gather
-    ga.g = d_grad_out;
-    ga.smap = smap;
-    ga.rden = rden;
-    ga.grad = d_grad_in;
-    ga.g_pitch = gout_pitch;
-    ga.grad_pitch = gin_pitch;
-    ga.W = width;
-    ga.H = height;
-    ga.D = ks->D;
-    ga.S = ks->S;
-    ga.blob = adj_blob;
-    ga.run_word = ks->adj_run_word;
-    ga.weight_word = ks->adj_weight_word;
+    ga->D = ks->D;
+    ga->S = ks->S;
+    ga->blob = adj_blob;
+    ga->run_word = ks->adj_run_word;
+    ga->weight_word = ks->adj_weight_word;
     const int nk = ks->D * ks->S;
     for (int k = 0; k < nk; k++) {
-        ga.rvar[k] = 1.0f / tab.var[k];
         // output rows [0, TH) read field rows ty + R + dy; output columns [0, TW) read field columns
         // tx + R + dx0 + [0, len + P - 1) for the thread's first output tx (a multiple of P)
         int ylo = 0, yhi = -1, xlo = 0, xhi = -1;
@@ -270,17 +259,59 @@ int adjoint_passes(const lpaici_kernelset *ks, const int *blob, const int *adj_b
             }
         }
         if (yhi < ylo) {
-            ga.rect[k] = make_int4(0, 0, 0, 0);  // no taps
+            ga->rect[k] = make_int4(0, 0, 0, 0);  // no taps
         } else {
-            const int col_end = std::min(ga.pitch, ga.R + kGatherTW + xhi + 1);
-            ga.rect[k] = make_int4(ga.R + ylo, ga.R + kGatherTH + yhi, (ga.R + xlo) >> 2, (col_end + 3) >> 2);
+            const int col_end = std::min(ga->pitch, ga->R + kGatherTW + xhi + 1);
+            ga->rect[k] = make_int4(ga->R + ylo, ga->R + kGatherTH + yhi, (ga->R + xlo) >> 2, (col_end + 3) >> 2);
         }
     }
     cudaError_t e = cudaFuncSetAttribute(lpaici_adjoint_gather_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem));
-    if (e != cudaSuccess) return cuda_error(e, "adjoint gather attributes");
-    lpaici_adjoint_gather_kernel<<<grid, kGatherThreads, smem, stream>>>(ga);
-    e = cudaGetLastError();
+                                         static_cast<int>(*smem));
+    return e == cudaSuccess ? LPAICI_OK : cuda_error(e, "adjoint gather attributes");
+}
+
+long gather_tiles(int width, int height, int *tiles_x) {
+    *tiles_x = (width + kGatherTW - 1) / kGatherTW;
+    return static_cast<long>(*tiles_x) * ((height + kGatherTH - 1) / kGatherTH);
+}
+
+}  // namespace
+
+// The two passes over caller-provided storage (lpaici_backward, lpaici_backward_noalloc).
+int adjoint_passes(const lpaici_kernelset *ks, const int *blob, const int *adj_blob, uint8_t *smap, float *rden,
+                   const float *d_noisy, int noisy_pitch, const float *d_grad_out, int gout_pitch, float *d_grad_in,
+                   int gin_pitch, int width, int height, float sigma, float gamma, cudaStream_t stream) {
+    GatherArgs ga{};
+    size_t smem = 0;
+    int rc = gather_setup(ks, adj_blob, &ga, &smem);
+    if (rc != LPAICI_OK) return rc;
+    int tiles_x = 0;
+    const long tiles = gather_tiles(width, height, &tiles_x);
+    if (tiles > 0x7fffffffL) return set_error(LPAICI_ERR_UNSUPPORTED, "image too large: %d x %d", width, height);
+
+    // A. selection
+    ImageArgs img{};
+    img.in = d_noisy;
+    img.out = nullptr;
+    img.smap = smap;
+    img.rden = rden;
+    img.W = width;
+    img.in_h = height;
+    img.in_pitch = noisy_pitch;
+    img.out_pitch = width;
+    img.row_begin = 0;
+    img.rows_out = height;
+    KernelTables tab;
+    fill_tables(ks, nullptr, sigma, gamma, &tab);
+    tab.blob = blob;
+    rc = launch_forward(ks, img, tab, default_config(ks), stream);
+    if (rc != LPAICI_OK) return rc;
+
+    // B. gather
+    ga.single = GatherImage{d_grad_out, smap, rden, d_grad_in, nullptr, gout_pitch, gin_pitch, width, height, tiles_x, 0};
+    for (int k = 0; k < ks->D * ks->S; k++) ga.rvar[k] = 1.0f / tab.var[k];
+    lpaici_adjoint_gather_kernel<<<static_cast<unsigned>(tiles), kGatherThreads, smem, stream>>>(ga);
+    const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? LPAICI_OK : cuda_error(e, "adjoint gather launch");
 }
 
@@ -378,4 +409,196 @@ extern "C" int lpaici_backward(const lpaici_kernelset *ks, const float *d_noisy,
     cudaError_t ef = cudaFreeAsync(ws, stream);
     if (rc == LPAICI_OK && ef != cudaSuccess) rc = cuda_error(ef, "cudaFreeAsync(adjoint workspace)");
     return rc;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Batched adjoint plan.
+// ---------------------------------------------------------------------------------------------
+struct lpaici_backward_batch {
+    int device = -1;
+    lpaici_batch *select = nullptr;  // pass A: the forward batch plan (out = null, s* and 1/den on)
+    void *dev_mem = nullptr;         // s* planes | 1/den maps | GatherImage[n] | 1/v tables | items
+    GatherArgs ga{};
+    size_t smem = 0;
+    unsigned grid = 0;
+    bool use_graph = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+int backward_batch_enqueue(lpaici_backward_batch *b, cudaStream_t stream) {
+    int rc = batch_plan_enqueue(b->select, stream);
+    if (rc != LPAICI_OK) return rc;
+    lpaici_adjoint_gather_kernel<<<b->grid, kGatherThreads, b->smem, stream>>>(b->ga);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? LPAICI_OK : cuda_error(e, "adjoint gather launch");
+}
+
+void backward_batch_free(lpaici_backward_batch *b) {
+    if (!b) return;
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    batch_plan_free(b->select);
+    if (b->dev_mem) cudaFree(b->dev_mem);
+    delete b;
+}
+
+size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
+
+}  // namespace
+
+extern "C" int lpaici_backward_batch_create(const lpaici_kernelset *ks, const lpaici_grad_image *images, int n,
+                                            const lpaici_batch_options *opts, lpaici_stream_t stream_,
+                                            lpaici_backward_batch **out) {
+    if (!ks || !images || n <= 0 || !out)
+        return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_backward_batch_create: bad argument");
+    *out = nullptr;
+    if (ks->S > 32) return set_error(LPAICI_ERR_UNSUPPORTED, "the adjoint supports at most 32 scales");
+    for (int i = 0; i < n; i++) {
+        const lpaici_grad_image &im = images[i];
+        if (!im.noisy || !im.grad_out || !im.grad_in || im.width <= 0 || im.height <= 0 || im.noisy_pitch < im.width ||
+            im.gout_pitch < im.width || im.gin_pitch < im.width)
+            return set_error(LPAICI_ERR_INVALID_ARG, "adjoint batch image %d: bad pointer, size or pitch", i);
+        if (!(im.sigma > 0.0f) || !(im.gamma > 0.0f))
+            return set_error(LPAICI_ERR_INVALID_ARG, "adjoint batch image %d: sigma and gamma need positive numbers",
+                             i);
+    }
+    cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+    const int *adj = nullptr;
+    int rc = device_adj_blob(ks, &adj);
+    if (rc != LPAICI_OK) return rc;
+    auto *b = new lpaici_backward_batch();
+    cudaGetDevice(&b->device);
+    rc = gather_setup(ks, adj, &b->ga, &b->smem);
+    if (rc != LPAICI_OK) {
+        backward_batch_free(b);
+        return rc;
+    }
+
+    // plan memory: per image s* planes and 1/den, then the gather's descriptors, tables and items
+    const int nk = ks->D * ks->S;
+    std::vector<size_t> smap_off(n), rden_off(n);
+    std::vector<int> tiles_x(n);
+    size_t off = 0;
+    long total_tiles = 0;
+    for (int i = 0; i < n; i++) {
+        const size_t npx = static_cast<size_t>(images[i].width) * images[i].height;
+        smap_off[i] = off;
+        off = align256(off + static_cast<size_t>(ks->D) * npx);
+        rden_off[i] = off;
+        off = align256(off + sizeof(float) * npx);
+        total_tiles += gather_tiles(images[i].width, images[i].height, &tiles_x[i]);
+    }
+    if (total_tiles > 0x7fffffffL) {
+        backward_batch_free(b);
+        return set_error(LPAICI_ERR_UNSUPPORTED, "adjoint batch too large: %ld tiles", total_tiles);
+    }
+    const size_t desc_off = off;
+    off = align256(off + sizeof(GatherImage) * n);
+    const size_t rvar_off = off;
+    off = align256(off + sizeof(float) * static_cast<size_t>(n) * nk);
+    const size_t item_off = off;
+    off = align256(off + sizeof(int2) * static_cast<size_t>(total_tiles));
+    cudaError_t e = cudaMalloc(&b->dev_mem, off);
+    if (e != cudaSuccess) {
+        backward_batch_free(b);
+        return cuda_error(e, "cudaMalloc(adjoint batch plan)");
+    }
+    char *base = static_cast<char *>(b->dev_mem);
+    std::vector<GatherImage> desc(n);
+    std::vector<float> rvar(static_cast<size_t>(n) * nk);
+    std::vector<int2> items;
+    items.reserve(static_cast<size_t>(total_tiles));
+    std::vector<BatchSpec> specs(n);
+    for (int i = 0; i < n; i++) {
+        const lpaici_grad_image &im = images[i];
+        uint8_t *smap = reinterpret_cast<uint8_t *>(base + smap_off[i]);
+        float *rden = reinterpret_cast<float *>(base + rden_off[i]);
+        KernelTables tab;
+        fill_tables(ks, nullptr, im.sigma, im.gamma, &tab);
+        float *rv = rvar.data() + static_cast<size_t>(i) * nk;
+        for (int k = 0; k < nk; k++) rv[k] = 1.0f / tab.var[k];
+        desc[i] = GatherImage{im.grad_out, smap, rden, im.grad_in,
+                              reinterpret_cast<const float *>(base + rvar_off) + static_cast<size_t>(i) * nk,
+                              im.gout_pitch, im.gin_pitch, im.width, im.height, tiles_x[i], 0};
+        int tx = 0;
+        const long t = gather_tiles(im.width, im.height, &tx);
+        for (long j = 0; j < t; j++) items.push_back(make_int2(i, static_cast<int>(j)));
+        specs[i] = BatchSpec{im.noisy, nullptr, smap, rden, im.width, im.height, im.noisy_pitch, im.width, im.sigma,
+                             im.gamma};
+    }
+    e = cudaMemcpy(base + desc_off, desc.data(), sizeof(GatherImage) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(base + rvar_off, rvar.data(), sizeof(float) * rvar.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(base + item_off, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        backward_batch_free(b);
+        return cuda_error(e, "cudaMemcpy(adjoint batch plan)");
+    }
+    b->ga.images = reinterpret_cast<const GatherImage *>(base + desc_off);
+    b->ga.items = reinterpret_cast<const int2 *>(base + item_off);
+    b->grid = static_cast<unsigned>(total_tiles);
+
+    const int config = (opts && opts->tile_config >= 0) ? opts->tile_config : default_config(ks);
+    rc = batch_plan_create(ks, specs.data(), n, config, false, stream, &b->select);
+    if (rc != LPAICI_OK) {
+        backward_batch_free(b);
+        return rc;
+    }
+    b->use_graph = opts && opts->use_graph;
+    if (b->use_graph) {
+        cudaStream_t cap = nullptr;
+        e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            rc = backward_batch_enqueue(b, cap);
+            const cudaError_t e2 = cudaStreamEndCapture(cap, &b->graph);
+            if (rc == LPAICI_OK && e2 != cudaSuccess) rc = cuda_error(e2, "cudaStreamEndCapture");
+            if (rc == LPAICI_OK) {
+                e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+                if (e != cudaSuccess) rc = cuda_error(e, "cudaGraphInstantiate");
+            }
+        } else {
+            rc = cuda_error(e, "graph capture");
+        }
+        if (cap) cudaStreamDestroy(cap);
+        if (rc == LPAICI_OK) {
+            e = cudaGraphUpload(b->exec, stream);
+            if (e != cudaSuccess) rc = cuda_error(e, "cudaGraphUpload");
+        }
+        if (rc != LPAICI_OK) {
+            backward_batch_free(b);
+            return rc;
+        }
+    }
+    *out = b;
+    return LPAICI_OK;
+}
+
+extern "C" int lpaici_backward_batch_run(lpaici_backward_batch *b, lpaici_stream_t stream_) {
+    if (!b) return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_backward_batch_run: null plan");
+    cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+    int dev = -1;
+    cudaGetDevice(&dev);
+    if (dev != b->device)
+        return set_error(LPAICI_ERR_INVALID_ARG, "adjoint batch planned on device %d, current device is %d", b->device,
+                         dev);
+    if (b->use_graph) {
+        const cudaError_t e = cudaGraphLaunch(b->exec, stream);
+        return e == cudaSuccess ? LPAICI_OK : cuda_error(e, "cudaGraphLaunch");
+    }
+    return backward_batch_enqueue(b, stream);
+}
+
+extern "C" int lpaici_backward_batch_destroy(lpaici_backward_batch *b) {
+    if (b) {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        cudaSetDevice(b->device);
+        cudaDeviceSynchronize();
+        backward_batch_free(b);
+        if (cur >= 0) cudaSetDevice(cur);
+    }
+    return LPAICI_OK;
 }

@@ -20,8 +20,9 @@ namespace lpaici {
 // Per-image descriptor in device memory.
 struct BatchImage {
     const float *in;
-    float *out;
+    float *out;       // null: no estimate (the adjoint's selection pass)
     uint8_t *smap;
+    float *rden;      // optional 1/den map (the adjoint's selection pass)
     int W, H, in_pitch, out_pitch;
     int tab_offset;  // float index of var[nk] (thr[nk] follows) in the plan's table array
     int pad;
@@ -71,6 +72,7 @@ __global__ void __launch_bounds__(32 * WX * WY, 1)
         img.in = bi.in;
         img.out = bi.out;
         img.smap = bi.smap;
+        img.rden = bi.rden;
         img.W = bi.W;
         img.in_h = bi.H;
         img.in_pitch = bi.in_pitch;
@@ -131,9 +133,9 @@ struct lpaici_batch {
     cudaGraphExec_t exec = nullptr;
 };
 
-namespace {
+namespace lpaici {
 
-int enqueue(lpaici_batch *b, cudaStream_t stream) {
+int batch_plan_enqueue(lpaici_batch *b, cudaStream_t stream) {
     cudaError_t e = cudaMemsetAsync(b->args.counter, 0, sizeof(unsigned), stream);
     if (e != cudaSuccess) return cuda_error(e, "cudaMemsetAsync(queue counter)");
     void *params[] = {&b->args};
@@ -142,7 +144,7 @@ int enqueue(lpaici_batch *b, cudaStream_t stream) {
     return LPAICI_OK;
 }
 
-void free_batch(lpaici_batch *b) {
+void batch_plan_free(lpaici_batch *b) {
     if (!b) return;
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
@@ -150,31 +152,18 @@ void free_batch(lpaici_batch *b) {
     delete b;
 }
 
-}  // namespace
-
-extern "C" {
-
-int lpaici_batch_create(const lpaici_kernelset *ks, const lpaici_image *images, int n, const lpaici_batch_options *opts,
-                        lpaici_stream_t stream_, lpaici_batch **out) {
-    if (!ks || !images || n <= 0 || !out) return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_batch_create: bad argument");
+// The plan of lpaici_batch_create for already validated images (specs); the adjoint's batched
+// selection pass uses it with out = null and smap/rden set.
+int batch_plan_create(const lpaici_kernelset *ks, const BatchSpec *specs, int n, int config, bool use_graph,
+                      cudaStream_t stream, lpaici_batch **out) {
     *out = nullptr;
-    cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
     const int nk = ks->D * ks->S;
     if (ks->S > kMaxScales)
         return set_error(LPAICI_ERR_UNSUPPORTED, "%d scales per direction; the kernels support at most %d", ks->S,
                          kMaxScales);
-    for (int i = 0; i < n; i++) {
-        const lpaici_image &im = images[i];
-        if (!im.noisy || !im.denoised || im.width <= 0 || im.height <= 0 || im.noisy_pitch < im.width ||
-            im.out_pitch < im.width)
-            return set_error(LPAICI_ERR_INVALID_ARG, "batch image %d: bad pointer or size", i);
-        if (!(im.sigma > 0.0f) || !(im.gamma > 0.0f))
-            return set_error(LPAICI_ERR_INVALID_ARG, "batch image %d: sigma and gamma need positive numbers", i);
-    }
     const int *blob = nullptr;
     int rc = device_blob(ks, &blob);
     if (rc != LPAICI_OK) return rc;
-    const int config = (opts && opts->tile_config >= 0) ? opts->tile_config : default_config(ks);
 
     auto *b = new lpaici_batch();
     cudaGetDevice(&b->device);
@@ -183,7 +172,7 @@ int lpaici_batch_create(const lpaici_kernelset *ks, const lpaici_image *images, 
     tab.blob = blob;
     rc = get_info(config, tab, &b->info);
     if (rc != LPAICI_OK) {
-        free_batch(b);
+        batch_plan_free(b);
         return rc;
     }
 
@@ -196,12 +185,12 @@ int lpaici_batch_create(const lpaici_kernelset *ks, const lpaici_image *images, 
     };
     std::vector<Item> items;
     for (int i = 0; i < n; i++) {
-        const lpaici_image &im = images[i];
+        const BatchSpec &im = specs[i];
         KernelTables t;
         fill_tables(ks, nullptr, im.sigma, im.gamma, &t);
         std::memcpy(&tables[static_cast<size_t>(i) * 2 * nk], t.var, sizeof(float) * nk);
         std::memcpy(&tables[static_cast<size_t>(i) * 2 * nk + nk], t.thr, sizeof(float) * nk);
-        imgs[i] = BatchImage{im.noisy, im.denoised, im.scale_map, im.width, im.height, im.noisy_pitch, im.out_pitch,
+        imgs[i] = BatchImage{im.noisy, im.out, im.smap, im.rden, im.width, im.height, im.noisy_pitch, im.out_pitch,
                              i * 2 * nk, 0};
         const int tx = (im.width + b->info.tile_w - 1) / b->info.tile_w;
         const int ty = (im.height + b->info.tile_h - 1) / b->info.tile_h;
@@ -227,7 +216,7 @@ int lpaici_batch_create(const lpaici_kernelset *ks, const lpaici_image *images, 
     const size_t total = ctr_off + 256;
     cudaError_t e = cudaMalloc(&b->dev_mem, total);
     if (e != cudaSuccess) {
-        free_batch(b);
+        batch_plan_free(b);
         return cuda_error(e, "cudaMalloc(batch plan)");
     }
     char *base = static_cast<char *>(b->dev_mem);
@@ -235,7 +224,7 @@ int lpaici_batch_create(const lpaici_kernelset *ks, const lpaici_image *images, 
     if (e == cudaSuccess) e = cudaMemcpy(base + tab_off, tables.data(), tab_bytes, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(base + item_off, qitems.data(), item_bytes, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
-        free_batch(b);
+        batch_plan_free(b);
         return cuda_error(e, "cudaMemcpy(batch plan)");
     }
     b->args.images = reinterpret_cast<const BatchImage *>(base);
@@ -256,7 +245,7 @@ int lpaici_batch_create(const lpaici_kernelset *ks, const lpaici_image *images, 
     cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
     if (b->info.smem > static_cast<size_t>(max_optin)) {
-        free_batch(b);
+        batch_plan_free(b);
         return set_error(LPAICI_ERR_UNSUPPORTED, "batched tile needs %zu B of shared memory, device allows %d",
                          b->info.smem, max_optin);
     }
@@ -264,19 +253,19 @@ int lpaici_batch_create(const lpaici_kernelset *ks, const lpaici_image *images, 
     if (e == cudaSuccess)
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, b->info.fn, b->info.threads, b->info.smem);
     if (e != cudaSuccess || per_sm <= 0) {
-        free_batch(b);
+        batch_plan_free(b);
         return e != cudaSuccess ? cuda_error(e, "batched occupancy")
                                 : set_error(LPAICI_ERR_UNSUPPORTED, "batched kernel does not fit on an SM");
     }
     b->grid = std::min(sms * per_sm, b->args.n_items);
 
-    b->use_graph = opts && opts->use_graph;
+    b->use_graph = use_graph;
     if (b->use_graph) {
         cudaStream_t cap = nullptr;
         e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
-            rc = enqueue(b, cap);
+            rc = batch_plan_enqueue(b, cap);
             cudaError_t e2 = cudaStreamEndCapture(cap, &b->graph);
             if (rc == LPAICI_OK && e2 != cudaSuccess) rc = cuda_error(e2, "cudaStreamEndCapture");
             if (rc == LPAICI_OK) {
@@ -288,17 +277,41 @@ int lpaici_batch_create(const lpaici_kernelset *ks, const lpaici_image *images, 
         }
         if (cap) cudaStreamDestroy(cap);
         if (rc != LPAICI_OK) {
-            free_batch(b);
+            batch_plan_free(b);
             return rc;
         }
         e = cudaGraphUpload(b->exec, stream);
         if (e != cudaSuccess) {
-            free_batch(b);
+            batch_plan_free(b);
             return cuda_error(e, "cudaGraphUpload");
         }
     }
     *out = b;
     return LPAICI_OK;
+}
+
+}  // namespace lpaici
+
+extern "C" {
+
+int lpaici_batch_create(const lpaici_kernelset *ks, const lpaici_image *images, int n, const lpaici_batch_options *opts,
+                        lpaici_stream_t stream_, lpaici_batch **out) {
+    if (!ks || !images || n <= 0 || !out) return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_batch_create: bad argument");
+    *out = nullptr;
+    std::vector<BatchSpec> specs(n);
+    for (int i = 0; i < n; i++) {
+        const lpaici_image &im = images[i];
+        if (!im.noisy || !im.denoised || im.width <= 0 || im.height <= 0 || im.noisy_pitch < im.width ||
+            im.out_pitch < im.width)
+            return set_error(LPAICI_ERR_INVALID_ARG, "batch image %d: bad pointer or size", i);
+        if (!(im.sigma > 0.0f) || !(im.gamma > 0.0f))
+            return set_error(LPAICI_ERR_INVALID_ARG, "batch image %d: sigma and gamma need positive numbers", i);
+        specs[i] = BatchSpec{im.noisy, im.denoised, im.scale_map, nullptr, im.width, im.height, im.noisy_pitch,
+                             im.out_pitch, im.sigma, im.gamma};
+    }
+    const int config = (opts && opts->tile_config >= 0) ? opts->tile_config : default_config(ks);
+    return batch_plan_create(ks, specs.data(), n, config, opts && opts->use_graph,
+                             reinterpret_cast<cudaStream_t>(stream_), out);
 }
 
 int lpaici_batch_run(lpaici_batch *b, lpaici_stream_t stream_) {
@@ -313,7 +326,7 @@ int lpaici_batch_run(lpaici_batch *b, lpaici_stream_t stream_) {
         if (e != cudaSuccess) return cuda_error(e, "cudaGraphLaunch");
         return LPAICI_OK;
     }
-    return enqueue(b, stream);
+    return batch_plan_enqueue(b, stream);
 }
 
 int lpaici_batch_destroy(lpaici_batch *b) {
@@ -322,7 +335,7 @@ int lpaici_batch_destroy(lpaici_batch *b) {
         cudaGetDevice(&cur);
         cudaSetDevice(b->device);
         cudaDeviceSynchronize();
-        free_batch(b);
+        batch_plan_free(b);
         if (cur >= 0) cudaSetDevice(cur);
     }
     return LPAICI_OK;
@@ -336,7 +349,7 @@ int lpaici_forward_batched(const lpaici_kernelset *ks, const lpaici_image *image
     rc = lpaici_batch_run(b, stream);
     cudaError_t e = cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream));
     if (rc == LPAICI_OK && e != cudaSuccess) rc = cuda_error(e, "cudaStreamSynchronize");
-    free_batch(b);
+    batch_plan_free(b);
     return rc;
 }
 

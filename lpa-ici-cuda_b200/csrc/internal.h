@@ -105,6 +105,20 @@ int launch_forward(const lpaici_kernelset *ks, const ImageArgs &img, const Kerne
 size_t config_smem(int config, int blob_words, int nk, int R);
 // The autotuned configuration of ks on the current device, else the first one that fits.
 int default_config(const lpaici_kernelset *ks);
+// One image of a batch plan (batched.cu): out may be null (no estimate), smap and rden optional.
+struct BatchSpec {
+    const float *noisy;
+    float *out;
+    uint8_t *smap;
+    float *rden;
+    int width, height, noisy_pitch, out_pitch;
+    float sigma, gamma;
+};
+int batch_plan_create(const lpaici_kernelset *ks, const BatchSpec *specs, int n, int config, bool use_graph,
+                      cudaStream_t stream, lpaici_batch **out);
+int batch_plan_enqueue(lpaici_batch *b, cudaStream_t stream);  // queue reset + persistent launch
+void batch_plan_free(lpaici_batch *b);
+
 // The adjoint's two passes over storage the caller provides: device copies of ks->blob and ks->adj_blob,
 // D*width*height selection bytes and width*height floats of 1/den.  Allocates nothing.
 int adjoint_passes(const lpaici_kernelset *ks, const int *blob, const int *adj_blob, uint8_t *smap, float *rden,

@@ -67,6 +67,14 @@ class BatchOptions(C.Structure):
     _fields_ = [("use_graph", C.c_int), ("tile_config", C.c_int)]
 
 
+class GradImage(C.Structure):
+    """lpaici_grad_image"""
+
+    _fields_ = [("noisy", C.c_void_p), ("grad_out", C.c_void_p), ("grad_in", C.c_void_p), ("width", C.c_int),
+                ("height", C.c_int), ("noisy_pitch", C.c_int), ("gout_pitch", C.c_int), ("gin_pitch", C.c_int),
+                ("sigma", C.c_float), ("gamma", C.c_float)]
+
+
 _vp, _i, _f, _fp, _ip = C.c_void_p, C.c_int, C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_int)
 _SIGS = {
     "lpaici_last_error": ([], C.c_char_p),
@@ -93,6 +101,10 @@ _SIGS = {
     "lpaici_backward": ([_vp, _vp, _i, _vp, _i, _vp, _i, _i, _i, _f, _f, _vp], _i),
     "lpaici_backward_noalloc": ([_vp, _vp, _i, _vp, _i, _vp, _i, _i, _i, _f, _f, _vp], _i),
     "lpaici_trim_workspace": ([], _i),
+    "lpaici_backward_batch_create": ([_vp, C.POINTER(GradImage), _i, C.POINTER(BatchOptions), _vp, C.POINTER(_vp)],
+                                     _i),
+    "lpaici_backward_batch_run": ([_vp, _vp], _i),
+    "lpaici_backward_batch_destroy": ([_vp], _i),
     "lpaici_anisotropic_gpu_fused": ([_fp, _fp, _i, _i, _i, _fp, _i, _i, _fp, _i, _ip, _ip, _ip, _fp, _f,
                                       C.POINTER(C.c_double)], _i),
     "lpaici_denoise_host": ([_vp, _fp, _fp, _i, _i, _f, _f, _vp], _i),
@@ -364,6 +376,50 @@ class Batch:
     def close(self) -> None:
         if self._h and self._h.value:
             _lib.lpaici_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class BackwardBatch:
+    """A planned batched adjoint (lpaici_backward_batch): selection of all images in one persistent
+    launch, gather of all images' tiles in one launch, optionally replayed from a CUDA graph."""
+
+    def __init__(self, ks: KernelSet, noisy: Sequence, grad_out: Sequence, grad_in: Sequence,
+                 sigmas: Sequence[float], gammas: Sequence[float], use_graph: bool = True, tile_config: int = -1):
+        import torch
+
+        n = len(noisy)
+        self._keep = (list(noisy), list(grad_out), list(grad_in))
+        arr = (GradImage * n)()
+        for i in range(n):
+            for t, name in ((noisy[i], "noisy"), (grad_out[i], "grad_out"), (grad_in[i], "grad_in")):
+                _check_image(t, f"{name}[{i}]")
+            H, W = noisy[i].shape
+            arr[i] = GradImage(noisy[i].data_ptr(), grad_out[i].data_ptr(), grad_in[i].data_ptr(), W, H,
+                               noisy[i].stride(0), grad_out[i].stride(0), grad_in[i].stride(0), float(sigmas[i]),
+                               float(gammas[i]))
+        opts = BatchOptions(1 if use_graph else 0, tile_config)
+        h = C.c_void_p()
+        self.device = noisy[0].device
+        with torch.cuda.device(self.device):
+            _check(_lib.lpaici_backward_batch_create(ks.handle, arr, n, C.byref(opts), _stream(torch), C.byref(h)),
+                   "lpaici_backward_batch_create")
+        self._h = h
+
+    def run(self) -> None:
+        import torch
+
+        with torch.cuda.device(self.device):
+            _check(_lib.lpaici_backward_batch_run(self._h, _stream(torch)), "lpaici_backward_batch_run")
+
+    def close(self) -> None:
+        if self._h and self._h.value:
+            _lib.lpaici_backward_batch_destroy(self._h)
             self._h = C.c_void_p()
 
     def __del__(self):

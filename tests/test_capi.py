@@ -73,3 +73,20 @@ def test_tile_configs_describe_all():
     assert len(cfgs) == lpaici.lib().lpaici_num_tile_configs() >= 3
     for tw, th, threads, ppt in cfgs:
         assert tw * th == threads * ppt  # every thread owns ppt pixels of the tile
+
+
+def test_backward_batch_arguments_checked_on_host():
+    """A null pointer or a bad size in any image is refused before any device work."""
+    lib = lpaici.lib()
+    arr = (lpaici.GradImage * 2)()
+    arr[0] = lpaici.GradImage(16, 16, 16, 4, 4, 4, 4, 4, 0.1, 2.0)
+    arr[1] = lpaici.GradImage(16, None, 16, 4, 4, 4, 4, 4, 0.1, 2.0)
+    ks = lpaici.KernelSet.load(__import__("conftest").kernel_file(__import__("conftest").SYM))
+    h = C.c_void_p()
+    assert lib.lpaici_backward_batch_create(ks.handle, arr, 2, None, None, C.byref(h)) == lpaici.ERR_INVALID_ARG
+    assert "image 1" in lib.lpaici_last_error().decode()
+    arr[1] = lpaici.GradImage(16, 16, 16, 4, 4, 3, 4, 4, 0.1, 2.0)  # noisy pitch < width
+    assert lib.lpaici_backward_batch_create(ks.handle, arr, 2, None, None, C.byref(h)) == lpaici.ERR_INVALID_ARG
+    arr[1] = lpaici.GradImage(16, 16, 16, 4, 4, 4, 4, 4, 0.0, 2.0)  # sigma 0
+    assert lib.lpaici_backward_batch_create(ks.handle, arr, 2, None, None, C.byref(h)) == lpaici.ERR_INVALID_ARG
+    assert lib.lpaici_backward_batch_destroy(None) == lpaici.OK
