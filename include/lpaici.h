@@ -258,7 +258,10 @@ int lpaici_anisotropic_gpu_fused(float *host_img_noisy, float *host_img_denoised
 
 /* Kernel-set form of the above: host in, host out, sigma/gamma, through device buffers cached
  * per thread and device (grown on demand, never shrunk; lpaici_release_host_buffers frees them).
- * Synchronises `stream` before returning. */
+ * The image goes through in row bands: the upload of a band's rows, its forward and its download
+ * run on separate streams, so with pinned host buffers the copies overlap the kernels; the result
+ * equals one full-image launch bit for bit.  Ordered after earlier work on `stream`; returns when
+ * the output is in host memory. */
 int lpaici_denoise_host(const lpaici_kernelset *ks, const float *host_noisy, float *host_denoised, int width,
                         int height, float sigma, float gamma, lpaici_stream_t stream);
 int lpaici_release_host_buffers(void);

@@ -1,5 +1,6 @@
 // capi.cu -- C ABI entry points for the forward path, the reference-shaped host engine and the
 // tile-configuration table.
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -117,10 +118,14 @@ int lpaici_tile_config_desc(int index, int *tile_w, int *tile_h, int *threads, i
 
 namespace {
 // Device buffers of lpaici_denoise_host, per thread and device.
+// Device buffers and the copy/compute pipeline of lpaici_denoise_host, per host thread and device.
+constexpr int kMaxBands = 64;
 struct HostBuffers {
     int dev = -1;
     float *in = nullptr, *out = nullptr;
     size_t cap = 0;
+    cudaStream_t s_in = nullptr, s_out = nullptr, s_comp[2] = {nullptr, nullptr};
+    cudaEvent_t ev_start = nullptr, ev_done = nullptr, ev_in[kMaxBands] = {}, ev_comp[kMaxBands] = {};
     ~HostBuffers() { release(); }
     void release() {
         if (dev >= 0) {
@@ -129,11 +134,34 @@ struct HostBuffers {
             cudaSetDevice(dev);
             cudaFree(in);
             cudaFree(out);
+            for (cudaStream_t st : {s_in, s_out, s_comp[0], s_comp[1]})
+                if (st) cudaStreamDestroy(st);
+            for (cudaEvent_t ev : {ev_start, ev_done})
+                if (ev) cudaEventDestroy(ev);
+            for (int i = 0; i < kMaxBands; i++) {
+                if (ev_in[i]) cudaEventDestroy(ev_in[i]);
+                if (ev_comp[i]) cudaEventDestroy(ev_comp[i]);
+                ev_in[i] = ev_comp[i] = nullptr;
+            }
             if (cur >= 0) cudaSetDevice(cur);
         }
         in = out = nullptr;
+        s_in = s_out = s_comp[0] = s_comp[1] = nullptr;
+        ev_start = ev_done = nullptr;
         cap = 0;
         dev = -1;
+    }
+    cudaError_t make_pipeline() {
+        cudaError_t e = cudaSuccess;
+        for (cudaStream_t *st : {&s_in, &s_out, &s_comp[0], &s_comp[1]})
+            if (e == cudaSuccess) e = cudaStreamCreateWithFlags(st, cudaStreamNonBlocking);
+        for (cudaEvent_t *ev : {&ev_start, &ev_done})
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+        for (int i = 0; i < kMaxBands && e == cudaSuccess; i++) {
+            e = cudaEventCreateWithFlags(&ev_in[i], cudaEventDisableTiming);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_comp[i], cudaEventDisableTiming);
+        }
+        return e;
     }
 };
 thread_local HostBuffers t_bufs;
@@ -147,27 +175,68 @@ int lpaici_denoise_host(const lpaici_kernelset *ks, const float *host_noisy, flo
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_error(e, "cudaGetDevice");
+    int rc = check_params(sigma, gamma);
+    if (rc != LPAICI_OK) return rc;
     const size_t n = static_cast<size_t>(width) * height;
     if (t_bufs.dev != dev || t_bufs.cap < n) {
         t_bufs.release();
+        t_bufs.dev = dev;
         e = cudaMalloc(&t_bufs.in, n * sizeof(float));
         if (e == cudaSuccess) e = cudaMalloc(&t_bufs.out, n * sizeof(float));
+        if (e == cudaSuccess) e = t_bufs.make_pipeline();
         if (e != cudaSuccess) {
             t_bufs.release();
-            return cuda_error(e, "cudaMalloc(host buffers)");
+            return cuda_error(e, "host-pointer buffers");
         }
-        t_bufs.dev = dev;
         t_bufs.cap = n;
     }
-    e = cudaMemcpyAsync(t_bufs.in, host_noisy, n * sizeof(float), cudaMemcpyHostToDevice, stream);
-    if (e != cudaSuccess) return cuda_error(e, "cudaMemcpyAsync(H2D)");
-    int rc = forward_common(ks, t_bufs.in, width, width, height, 0, height, t_bufs.out, width, nullptr, sigma, gamma,
-                            nullptr, stream);
+    // Row bands, pipelined: the upload of the rows band b needs (its rows + R below) on s_in, its
+    // forward on one of two compute streams (the next band's CTAs fill the SMs while this band's last
+    // wave drains), its download on s_out.  With pinned host buffers the copies overlap the kernels.
+    int tile_h = 64;
+    lpaici_tile_config_desc(default_config(ks), nullptr, &tile_h, nullptr, nullptr);
+    const int R = ks->radius;
+    int band = ((height + 7) / 8 + tile_h - 1) / tile_h * tile_h;
+    if (band < tile_h) band = tile_h;
+    while ((height + band - 1) / band > kMaxBands) band += tile_h;
+    const int nb = (height + band - 1) / band;
+    HostBuffers &b = t_bufs;
+    e = cudaEventRecord(b.ev_start, stream);
+    for (cudaStream_t st : {b.s_in, b.s_out, b.s_comp[0], b.s_comp[1]})
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(st, b.ev_start, 0);
+    if (e != cudaSuccess) return cuda_error(e, "lpaici_denoise_host: stream order");
+    int copied = 0;  // input rows [0, copied) uploaded
+    for (int i = 0; i < nb && rc == LPAICI_OK; i++) {
+        const int r0 = i * band, r1 = std::min(height, r0 + band), need = std::min(height, r1 + R);
+        if (need > copied) {
+            e = cudaMemcpyAsync(b.in + static_cast<size_t>(copied) * width, host_noisy + static_cast<size_t>(copied) * width,
+                                sizeof(float) * width * static_cast<size_t>(need - copied), cudaMemcpyHostToDevice, b.s_in);
+            copied = need;
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(b.ev_in[i], b.s_in);
+        cudaStream_t sc = b.s_comp[i & 1];
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(sc, b.ev_in[i], 0);
+        if (e != cudaSuccess) {
+            rc = cuda_error(e, "lpaici_denoise_host: upload");
+            break;
+        }
+        rc = forward_common(ks, b.in, width, width, height, r0, r1 - r0, b.out + static_cast<size_t>(r0) * width, width,
+                            nullptr, sigma, gamma, nullptr, sc);
+        if (rc != LPAICI_OK) break;
+        e = cudaEventRecord(b.ev_comp[i], sc);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(b.s_out, b.ev_comp[i], 0);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(host_denoised + static_cast<size_t>(r0) * width, b.out + static_cast<size_t>(r0) * width,
+                                sizeof(float) * width * static_cast<size_t>(r1 - r0), cudaMemcpyDeviceToHost, b.s_out);
+        if (e != cudaSuccess) rc = cuda_error(e, "lpaici_denoise_host: download");
+    }
+    // every band's download waited for its forward, every forward for its upload: s_out covers all
+    e = cudaEventRecord(b.ev_done, b.s_out);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(stream, b.ev_done, 0);
+    const cudaError_t es = cudaStreamSynchronize(b.s_out);
     if (rc != LPAICI_OK) return rc;
-    e = cudaMemcpyAsync(host_denoised, t_bufs.out, n * sizeof(float), cudaMemcpyDeviceToHost, stream);
-    if (e != cudaSuccess) return cuda_error(e, "cudaMemcpyAsync(D2H)");
-    e = cudaStreamSynchronize(stream);
-    if (e != cudaSuccess) return cuda_error(e, "cudaStreamSynchronize");
+    if (e != cudaSuccess) return cuda_error(e, "lpaici_denoise_host: join");
+    if (es != cudaSuccess) return cuda_error(es, "cudaStreamSynchronize");
     return LPAICI_OK;
 }
 

@@ -206,3 +206,20 @@ def test_error_against_fp64():
     assert np.abs(out.astype(np.float64) - o64)[same].max() <= 2e-6
     psnr64 = 10.0 * np.log10(1.0 / np.mean((clean.astype(np.float64) - o64) ** 2))
     assert abs(lpaici.psnr(clean, out) - psnr64) <= 0.01
+
+
+@pytest.mark.parametrize("W,H", [(1000, 1500), (517, 81), (33, 1), (2048, 4097)])
+def test_host_engine_bands_equal_device_path(W, H):
+    """lpaici_denoise_host pipelines row bands (upload, forward, download on separate streams); its
+    result equals the single device launch bit for bit, from pageable and from pinned host buffers."""
+    import torch
+
+    ks = lpaici.KernelSet.load(kernel_file(SYM))
+    noisy = lpaici.add_noise(lpaici.synth_image(W, H, 7), SIGMA_20, 11)
+    ref = lpaici.forward(ks, torch.from_numpy(noisy).cuda(), SIGMA_20, 2.0).cpu().numpy()
+    got = lpaici.denoise_host(ks, noisy, SIGMA_20, 2.0)
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+    pin_in = torch.from_numpy(noisy).pin_memory()
+    pin_out = torch.empty_like(pin_in).pin_memory()
+    lpaici.denoise_host(ks, pin_in.numpy(), SIGMA_20, 2.0, out=pin_out.numpy())
+    assert np.array_equal(pin_out.numpy().view(np.uint32), ref.view(np.uint32))
