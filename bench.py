@@ -10,7 +10,8 @@ rank's time.
   value     Mpix/s with the input resident in HBM, device time of the forward launch (CUDA events on
             the launching stream), L2 flushed (256 MB write) between timed steps
   e2e       the same metric through the C ABI's host-pointer entry (lpaici_denoise_host): pinned host
-            input -> H2D -> forward -> D2H -> host, synchronous, wall clock per step
+            input -> H2D -> forward -> D2H -> host (row bands, copies overlapped with the kernels on
+            separate streams), returns when the output is in host memory, wall clock per step
   roofline  FP32 bound: every tap is one multiply and one separately rounded add (bit-exact with the
             reference), so the peak is the FP32 pipe's measured rate for exactly that (probe in
             lib/liblpaici_bench.so, the faster of scalar FMUL+FADD and packed fma(w,x,-0)+add);
