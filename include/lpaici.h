@@ -32,7 +32,7 @@ extern "C" {
 
 /* ---- status codes ------------------------------------------------------------------------- */
 #define LPAICI_OK 0
-#define LPAICI_ERR_INVALID_ARG 1    /* null pointer, size <= 0, sigma/gamma not > 0, channels != 1 ... */
+#define LPAICI_ERR_INVALID_ARG 1    /* null pointer, size <= 0, sigma/gamma not > 0, channels outside 1..64 ... */
 #define LPAICI_ERR_FILE 2           /* a file cannot be opened / read / written */
 #define LPAICI_ERR_KERNEL_FORMAT 3  /* malformed kernel file or kernel arrays */
 #define LPAICI_ERR_UNSUPPORTED 4    /* valid input beyond this build's limits (e.g. kernel radius) */
@@ -133,6 +133,15 @@ int lpaici_forward_var(const lpaici_kernelset *ks, const float *d_noisy, int noi
 int lpaici_forward_rows(const lpaici_kernelset *ks, const float *d_in, int in_pitch, int width, int in_height,
                         int row_begin, int row_count, float *d_out, int out_pitch, float sigma, float gamma,
                         uint8_t *d_scale_map, lpaici_stream_t stream);
+
+/* An image of `channels` interleaved channels (pixel x of row y, channel c at float y * pitch +
+ * x * channels + c; pitches in floats, >= width * channels), every channel denoised on its own with
+ * the same sigma and gamma, read and written in place with element stride `channels`.  The
+ * reference's engine takes a channel count but implements one channel (its main converts every
+ * image to gray); here channel c of the result equals the single-channel forward of channel c. */
+int lpaici_forward_channels(const lpaici_kernelset *ks, const float *d_noisy, int noisy_pitch, float *d_denoised,
+                            int out_pitch, int width, int height, int channels, float sigma, float gamma,
+                            lpaici_stream_t stream);
 
 /* ---- batched forward: images of uneven sizes, sigmas and gammas in one persistent launch ----- */
 typedef struct {
@@ -246,7 +255,8 @@ int lpaici_backward_noalloc(const lpaici_kernelset *ks, const float *d_noisy, in
 /* The reference engine's own signature and ownership (anisotropic_lpa_ici_gpu_fused,
  * src/v4_1_lpa_ici_2D_sparse_shared.cu:1122-1244): host input and output buffers, the dense
  * kernels and the caller's variances; copies in, denoises on the current device, copies out,
- * synchronously.  channels must be 1; host_global_weights_buffer is unused (may be NULL), as on the
+ * synchronously.  channels: 1, or up to 64 interleaved channels denoised one by one (the reference
+ * implements one; lpaici_forward_channels); host_global_weights_buffer is unused (may be NULL), as on the
  * reference's GPU path.  *seconds, if not NULL, receives the reference's timing window: from
  * after the uploads to after the copy of the result back to the host (:1216-1240).
  * Errors are returned instead of exiting the process. */

@@ -37,11 +37,12 @@ static int check_params(float sigma_or_one, float gamma) {
 // Shared body of the forward entry points.
 static int forward_common(const lpaici_kernelset *ks, const float *d_in, int in_pitch, int width, int in_height,
                           int row_begin, int row_count, float *d_out, int out_pitch, const float *host_var,
-                          float sigma, float gamma, uint8_t *d_smap, cudaStream_t stream) {
+                          float sigma, float gamma, uint8_t *d_smap, cudaStream_t stream, int step = 1) {
     if (!ks || !d_in || !d_out) return set_error(LPAICI_ERR_INVALID_ARG, "forward: null kernel set or image pointer");
     if (width <= 0 || in_height <= 0 || row_count <= 0)
         return set_error(LPAICI_ERR_INVALID_ARG, "forward: non-positive size %d x %d", width, row_count);
-    if (in_pitch < width || out_pitch < width)
+    const long row_floats = static_cast<long>(width - 1) * step + 1;
+    if (in_pitch < row_floats || out_pitch < row_floats)
         return set_error(LPAICI_ERR_INVALID_ARG, "forward: pitch smaller than width");
     if (row_begin < 0 || row_begin + row_count > in_height)
         return set_error(LPAICI_ERR_INVALID_ARG, "forward: output rows [%d, %d) outside the %d input rows", row_begin,
@@ -65,10 +66,27 @@ static int forward_common(const lpaici_kernelset *ks, const float *d_in, int in_
     img.out_pitch = out_pitch;
     img.row_begin = row_begin;
     img.rows_out = row_count;
+    img.step = step;
     KernelTables tab;
     fill_tables(ks, host_var, sigma, gamma, &tab);
     tab.blob = blob;
     return launch_forward(ks, img, tab, default_config(ks), stream);
+}
+
+// Every channel of an interleaved image (pixel (x, y), channel c at row y, float x * channels + c) as
+// its own image, in place: one launch per channel with element stride `channels`.
+static int forward_channels(const lpaici_kernelset *ks, const float *d_in, int in_pitch, float *d_out, int out_pitch,
+                            int width, int height, int channels, const float *host_var, float sigma, float gamma,
+                            cudaStream_t stream) {
+    if (channels <= 0 || channels > 64)
+        return set_error(LPAICI_ERR_INVALID_ARG, "channels must be 1 .. 64, got %d", channels);
+    for (int c = 0; c < channels; c++) {
+        const int rc = forward_common(ks, d_in ? d_in + c : nullptr, in_pitch, width, height, 0, height,
+                                      d_out ? d_out + c : nullptr, out_pitch, host_var, sigma, gamma, nullptr, stream,
+                                      channels);
+        if (rc != LPAICI_OK) return rc;
+    }
+    return LPAICI_OK;
 }
 
 }  // namespace lpaici
@@ -95,6 +113,13 @@ int lpaici_forward_rows(const lpaici_kernelset *ks, const float *d_in, int in_pi
                         uint8_t *d_scale_map, lpaici_stream_t stream) {
     return forward_common(ks, d_in, in_pitch, width, in_height, row_begin, row_count, d_out, out_pitch, nullptr, sigma,
                           gamma, d_scale_map, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int lpaici_forward_channels(const lpaici_kernelset *ks, const float *d_noisy, int noisy_pitch, float *d_denoised,
+                            int out_pitch, int width, int height, int channels, float sigma, float gamma,
+                            lpaici_stream_t stream) {
+    return forward_channels(ks, d_noisy, noisy_pitch, d_denoised, out_pitch, width, height, channels, nullptr, sigma,
+                            gamma, reinterpret_cast<cudaStream_t>(stream));
 }
 
 int lpaici_num_tile_configs(void) { return LPAICI_NUM_TILE_CONFIGS; }
@@ -251,7 +276,8 @@ int lpaici_anisotropic_gpu_fused(float *host_img_noisy, float *host_img_denoised
                                  int *host_rows, int *host_cols, float *host_kernel_variances, float ici_gamma,
                                  double *seconds) {
     (void)host_global_weights_buffer;
-    if (channels != 1) return set_error(LPAICI_ERR_INVALID_ARG, "channels must be 1, got %d", channels);
+    if (channels <= 0 || channels > 64)
+        return set_error(LPAICI_ERR_INVALID_ARG, "channels must be 1 .. 64, got %d", channels);
     if (!host_img_noisy || !host_img_denoised || !host_kernel_weights || !host_offsets || !host_rows || !host_cols ||
         !host_kernel_variances || width <= 0 || height <= 0)
         return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_anisotropic_gpu_fused: bad argument");
@@ -264,7 +290,7 @@ int lpaici_anisotropic_gpu_fused(float *host_img_noisy, float *host_img_denoised
     lpaici_kernelset *ks = nullptr;
     int rc = lpaici_kernelset_create(host_kernel_weights, host_offsets, host_rows, host_cols, num_dirs, num_scales, &ks);
     if (rc != LPAICI_OK) return rc;
-    const size_t n = static_cast<size_t>(width) * height;
+    const size_t n = static_cast<size_t>(width) * height * channels;
     float *d_in = nullptr, *d_out = nullptr;
     cudaError_t e = cudaMalloc(&d_in, n * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc(&d_out, n * sizeof(float));
@@ -274,8 +300,8 @@ int lpaici_anisotropic_gpu_fused(float *host_img_noisy, float *host_img_denoised
     } else {
         cudaDeviceSynchronize();
         const auto t0 = std::chrono::steady_clock::now();  // the reference's window starts here (:1216)
-        rc = forward_common(ks, d_in, width, width, height, 0, height, d_out, width, host_kernel_variances, 1.0f,
-                            ici_gamma, nullptr, nullptr);
+        rc = forward_channels(ks, d_in, width * channels, d_out, width * channels, width, height, channels,
+                              host_kernel_variances, 1.0f, ici_gamma, nullptr);
         if (rc == LPAICI_OK) {
             e = cudaMemcpy(host_img_denoised, d_out, n * sizeof(float), cudaMemcpyDeviceToHost);
             if (e != cudaSuccess) rc = cuda_error(e, "cudaMemcpy(D2H)");

@@ -45,6 +45,7 @@ struct ImageArgs {
     int W, in_h, in_pitch, out_pitch;
     int row_begin;    // output row r is input row row_begin + r
     int rows_out;
+    int step = 1;     // floats between neighbouring pixels of a row, in and out (channels of an interleaved image)
 };
 
 struct KernelTables {

@@ -166,7 +166,8 @@ __device__ __forceinline__ void load_tile(float2 *s_tile, const ImageArgs &img, 
         for (int c = lane; c < g.pitch2; c += 32) {
             const int gx = gx0 + c;
             const bool ok_x = gx >= 0 && gx < img.W;
-            dst[c] = make_float2(ok_a && ok_x ? __ldg(ra + gx) : 0.0f, ok_b && ok_x ? __ldg(rb + gx) : 0.0f);
+            const size_t at = static_cast<size_t>(gx) * img.step;
+            dst[c] = make_float2(ok_a && ok_x ? __ldg(ra + at) : 0.0f, ok_b && ok_x ? __ldg(rb + at) : 0.0f);
         }
     }
 }
@@ -291,7 +292,8 @@ __device__ __forceinline__ void sweep_tile(const ImageArgs &img, int x0, int y0,
 #pragma unroll
         for (int i = 0; i < 2 * Q; i++)
             if (valid & (1u << i))
-                img.out[static_cast<size_t>(oy + 8 * (i & 1)) * img.out_pitch + ox + (i >> 1)] =
+                img.out[static_cast<size_t>(oy + 8 * (i & 1)) * img.out_pitch +
+                        static_cast<size_t>(ox + (i >> 1)) * img.step] =
                     __fdiv_rn(pick<Q>(num, i), pick<Q>(den, i));
     }
     if (img.rden) {

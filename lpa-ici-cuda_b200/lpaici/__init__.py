@@ -101,6 +101,7 @@ _SIGS = {
     "lpaici_backward": ([_vp, _vp, _i, _vp, _i, _vp, _i, _i, _i, _f, _f, _vp], _i),
     "lpaici_backward_noalloc": ([_vp, _vp, _i, _vp, _i, _vp, _i, _i, _i, _f, _f, _vp], _i),
     "lpaici_trim_workspace": ([], _i),
+    "lpaici_forward_channels": ([_vp, _vp, _i, _vp, _i, _i, _i, _i, _f, _f, _vp], _i),
     "lpaici_backward_batch_create": ([_vp, C.POINTER(GradImage), _i, C.POINTER(BatchOptions), _vp, C.POINTER(_vp)],
                                      _i),
     "lpaici_backward_batch_run": ([_vp, _vp], _i),
@@ -321,6 +322,25 @@ def forward_rows(ks: KernelSet, band, row_begin: int, row_count: int, sigma: flo
                                       row_count, C.c_void_p(out.data_ptr()), out.stride(0), sigma, gamma, sp,
                                       _stream(torch))
     _check(rc, "lpaici_forward_rows")
+    return out
+
+
+def forward_channels(ks: KernelSet, noisy, sigma: float, gamma: float, out=None):
+    """Denoises every channel of an interleaved H x W x C image (CUDA float32, rows contiguous within
+    themselves) on its own: lpaici_forward_channels."""
+    import torch
+
+    if noisy.dim() != 3 or noisy.dtype != torch.float32 or not noisy.is_cuda or noisy.stride(2) != 1 or \
+            noisy.stride(1) != noisy.shape[2]:
+        raise ValueError("noisy: a CUDA float32 H x W x C tensor with interleaved channels")
+    H, W, Cn = noisy.shape
+    if out is None:
+        out = torch.empty_like(noisy)
+    with torch.cuda.device(noisy.device):
+        rc = _lib.lpaici_forward_channels(ks.handle, C.c_void_p(noisy.data_ptr()), noisy.stride(0),
+                                          C.c_void_p(out.data_ptr()), out.stride(0), W, H, Cn, sigma, gamma,
+                                          _stream(torch))
+    _check(rc, "lpaici_forward_channels")
     return out
 
 

@@ -53,7 +53,8 @@ def test_null_arguments_rejected():
 
 
 def test_reference_engine_argument_checks():
-    """channels != 1 and kernels outside the weight array are refused before any device work."""
+    """A channel count outside 1..64 and kernels outside the weight array are refused before any device
+    work."""
     w = np.ones(9, np.float32)
     off, rows, cols = (np.array([v], np.int32) for v in (0, 3, 3))
     x = np.zeros((4, 4), np.float32)
@@ -64,7 +65,8 @@ def test_reference_engine_argument_checks():
     args = lambda ch, size: (x.ctypes.data_as(fp), x.copy().ctypes.data_as(fp), 4, 4, ch, None, 1, 1,
                              w.ctypes.data_as(fp), size, off.ctypes.data_as(ip), rows.ctypes.data_as(ip),
                              cols.ctypes.data_as(ip), var.ctypes.data_as(fp), 2.0, None)
-    assert lib.lpaici_anisotropic_gpu_fused(*args(3, 9)) == lpaici.ERR_INVALID_ARG
+    assert lib.lpaici_anisotropic_gpu_fused(*args(0, 9)) == lpaici.ERR_INVALID_ARG
+    assert lib.lpaici_anisotropic_gpu_fused(*args(65, 9)) == lpaici.ERR_INVALID_ARG
     assert lib.lpaici_anisotropic_gpu_fused(*args(1, 8)) == lpaici.ERR_KERNEL_FORMAT
 
 
