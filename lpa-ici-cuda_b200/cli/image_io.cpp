@@ -5,6 +5,7 @@
 
 #include <zlib.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -87,7 +88,7 @@ inline int sample(const uint8_t *row, int x, int ch, int channels, int depth) {
     return (row[idx / per] >> shift) & ((1 << depth) - 1);
 }
 
-bool load_png(const std::vector<uint8_t> &f, std::vector<float> &img, int &W, int &H, std::string &err) {
+bool load_png(const std::vector<uint8_t> &f, std::vector<float> &img, int &W, int &H, int comps, std::string &err) {
     if (f.size() < 8 + 25) return err = "truncated PNG", false;
     size_t pos = 8;
     int depth = 0, ctype = -1, interlace = 0;
@@ -148,32 +149,44 @@ bool load_png(const std::vector<uint8_t> &f, std::vector<float> &img, int &W, in
     if (uncompress(raw.data(), &raw_len, idat.data(), static_cast<uLong>(idat.size())) != Z_OK)
         return err = "corrupt PNG data", false;
 
-    // 8-bit gray per pixel (16-bit samples: gray conversion at 16 bits, then the high byte)
-    std::vector<uint8_t> gray(static_cast<size_t>(W) * H);
+    // 8-bit samples per pixel: gray (comps 1; 16-bit samples: gray conversion at 16 bits, then the
+    // high byte) or R, G, B (comps 3; gray replicated, alpha dropped, 16-bit samples' high bytes)
+    std::vector<uint8_t> gray(static_cast<size_t>(W) * H * comps);
     static const int scale[9] = {0, 0xff, 0x55, 0, 0x11, 0, 0, 0, 0x01};
     auto put_row = [&](const uint8_t *row, int n, int y, int x0, int dx) {
         for (int i = 0; i < n; i++) {
-            uint8_t g;
+            int rgb[3] = {0, 0, 0}, g = 0;
+            bool color = false;
             if (ctype == 3) {
                 const int idx = sample(row, i, 0, 1, depth);
-                if (3 * idx + 2 >= static_cast<int>(plte.size())) {
-                    g = 0;
-                } else {
-                    g = luma(plte[3 * idx], plte[3 * idx + 1], plte[3 * idx + 2]);
-                }
+                if (3 * idx + 2 < static_cast<int>(plte.size()))
+                    for (int k = 0; k < 3; k++) rgb[k] = plte[3 * idx + k];
+                color = true;
             } else if (depth == 16) {
-                int v;
-                if (channels >= 3) v = luma16(sample(row, i, 0, channels, 16), sample(row, i, 1, channels, 16),
-                                              sample(row, i, 2, channels, 16));
-                else v = sample(row, i, 0, channels, 16);
-                g = static_cast<uint8_t>((v >> 8) & 0xff);
+                if (channels >= 3) {
+                    for (int k = 0; k < 3; k++) rgb[k] = sample(row, i, k, channels, 16);
+                    if (comps == 1) {
+                        g = (luma16(rgb[0], rgb[1], rgb[2]) >> 8) & 0xff;
+                    } else {
+                        for (int k = 0; k < 3; k++) rgb[k] >>= 8;
+                        color = true;
+                    }
+                } else {
+                    g = (sample(row, i, 0, channels, 16) >> 8) & 0xff;
+                }
             } else if (channels >= 3) {
-                g = luma(sample(row, i, 0, channels, 8), sample(row, i, 1, channels, 8), sample(row, i, 2, channels, 8));
+                for (int k = 0; k < 3; k++) rgb[k] = sample(row, i, k, channels, 8);
+                color = true;
             } else {
                 const int v = sample(row, i, 0, channels, depth);
-                g = static_cast<uint8_t>(depth < 8 ? v * scale[depth] : v);
+                g = depth < 8 ? v * scale[depth] : v;
             }
-            gray[static_cast<size_t>(y) * W + x0 + static_cast<size_t>(i) * dx] = g;
+            uint8_t *dst = &gray[(static_cast<size_t>(y) * W + x0 + static_cast<size_t>(i) * dx) * comps];
+            if (comps == 1) {
+                dst[0] = static_cast<uint8_t>(color ? luma(rgb[0], rgb[1], rgb[2]) : g);
+            } else {
+                for (int k = 0; k < 3; k++) dst[k] = static_cast<uint8_t>(color ? rgb[k] : g);
+            }
         }
     };
     if (interlace == 0) {
@@ -204,7 +217,7 @@ bool load_png(const std::vector<uint8_t> &f, std::vector<float> &img, int &W, in
     return true;
 }
 
-bool load_pgm(const std::vector<uint8_t> &f, std::vector<float> &img, int &W, int &H, std::string &err) {
+bool load_pgm(const std::vector<uint8_t> &f, std::vector<float> &img, int &W, int &H, int comps, std::string &err) {
     size_t pos = 2;
     int vals[3] = {0, 0, 0}, n = 0;
     while (n < 3 && pos < f.size()) {
@@ -225,19 +238,28 @@ bool load_pgm(const std::vector<uint8_t> &f, std::vector<float> &img, int &W, in
     if (n < 3 || W <= 0 || H <= 0 || vals[2] != 255) return err = "unsupported PGM (8-bit P5 only)", false;
     if (f.size() < pos + static_cast<size_t>(W) * H) return err = "truncated PGM", false;
     const float *lut = ldr_to_float_table();
-    img.resize(static_cast<size_t>(W) * H);
-    for (size_t i = 0; i < img.size(); i++) img[i] = lut[f[pos + i]];
+    img.resize(static_cast<size_t>(W) * H * comps);
+    for (size_t i = 0; i < img.size(); i++) img[i] = lut[f[pos + i / comps]];
     return true;
 }
 
-// RGBE pixel to gray: (R + G + B) * 2^(E - 136) / 3 in float, 0 when E == 0.
+// RGBE pixel to gray: (R + G + B) * 2^(E - 136) / 3 in float, 0 when E == 0; to RGB: each
+// mantissa byte times 2^(E - 136).
 inline float rgbe_gray(const uint8_t *p) {
     if (p[3] == 0) return 0.0f;
     const float f1 = static_cast<float>(std::ldexp(1.0f, p[3] - static_cast<int>(128 + 8)));
     return (p[0] + p[1] + p[2]) * f1 / 3;
 }
+inline void rgbe_decode(const uint8_t *p, int comps, float *out) {
+    if (comps == 1) {
+        out[0] = rgbe_gray(p);
+        return;
+    }
+    const float f1 = p[3] ? static_cast<float>(std::ldexp(1.0f, p[3] - static_cast<int>(128 + 8))) : 0.0f;
+    for (int k = 0; k < 3; k++) out[k] = p[3] ? p[k] * f1 : 0.0f;
+}
 
-bool load_hdr(const std::vector<uint8_t> &f, std::vector<float> &img, int &W, int &H, std::string &err) {
+bool load_hdr(const std::vector<uint8_t> &f, std::vector<float> &img, int &W, int &H, int comps, std::string &err) {
     size_t pos = 0;
     auto line = [&]() {
         std::string s;
@@ -258,11 +280,11 @@ bool load_hdr(const std::vector<uint8_t> &f, std::vector<float> &img, int &W, in
     const std::string dims = line();
     if (std::sscanf(dims.c_str(), "-Y %d +X %d", &H, &W) != 2 || W <= 0 || H <= 0 || W > (1 << 24) || H > (1 << 24))
         return err = "unsupported HDR orientation or size", false;
-    img.assign(static_cast<size_t>(W) * H, 0.0f);
+    img.assign(static_cast<size_t>(W) * H * comps, 0.0f);
     auto flat = [&](size_t from_px) {
-        for (size_t i = from_px; i < img.size(); i++) {
+        for (size_t i = from_px; i < static_cast<size_t>(W) * H; i++) {
             if (pos + 4 > f.size()) return false;
-            img[i] = rgbe_gray(&f[pos]);
+            rgbe_decode(&f[pos], comps, &img[i * comps]);
             pos += 4;
         }
         return true;
@@ -298,22 +320,27 @@ bool load_hdr(const std::vector<uint8_t> &f, std::vector<float> &img, int &W, in
                 }
             }
         }
-        for (int x = 0; x < W; x++) img[static_cast<size_t>(y) * W + x] = rgbe_gray(&scan[4 * x]);
+        for (int x = 0; x < W; x++) rgbe_decode(&scan[4 * x], comps, &img[(static_cast<size_t>(y) * W + x) * comps]);
     }
     return true;
 }
 
-// Gray value to RGBE with R = G = B: mantissa = v * (frexp(v) * 256 / v), truncated to 8 bits.
-inline void gray_rgbe(float v, uint8_t *out) {
-    if (v < 1e-32f) {
+// Linear R, G, B to RGBE: with m = max(R, G, B), every channel's mantissa is c * (frexp(m) * 256 / m)
+// truncated to 8 bits, the exponent frexp's + 128; all zero when m < 1e-32.  Gray is R = G = B.
+inline void rgb_rgbe(const float *c, uint8_t *out) {
+    const float m = std::max(std::max(c[0], c[1]), c[2]);
+    if (m < 1e-32f) {
         out[0] = out[1] = out[2] = out[3] = 0;
         return;
     }
     int e = 0;
-    const float normalize = static_cast<float>(std::frexp(v, &e)) * 256.0f / v;
-    const uint8_t m = static_cast<uint8_t>(v * normalize);
-    out[0] = out[1] = out[2] = m;
+    const float normalize = static_cast<float>(std::frexp(m, &e)) * 256.0f / m;
+    for (int k = 0; k < 3; k++) out[k] = static_cast<uint8_t>(c[k] * normalize);
     out[3] = static_cast<uint8_t>(e + 128);
+}
+inline void pixel_rgbe(const float *px, int comps, uint8_t *out) {
+    const float c[3] = {px[0], px[comps == 1 ? 0 : 1], px[comps == 1 ? 0 : 2]};
+    rgb_rgbe(c, out);
 }
 
 // Radiance run-length coding of one component line: runs of >= 3 equal bytes as (128 + n, byte),
@@ -356,18 +383,24 @@ const float *ldr_to_float_table() {
     return table;
 }
 
-bool load_gray(const std::string &path, std::vector<float> &img, int &width, int &height, std::string &err) {
+bool load_image(const std::string &path, int comps, std::vector<float> &img, int &width, int &height,
+                std::string &err) {
+    if (comps != 1 && comps != 3) return err = "1 or 3 channels", false;
     std::vector<uint8_t> f;
     if (!read_file(path, f)) return err = "cannot open file", false;
     static const uint8_t png_sig[8] = {0x89, 'P', 'N', 'G', '\r', '\n', 0x1a, '\n'};
-    if (f.size() >= 8 && !std::memcmp(f.data(), png_sig, 8)) return load_png(f, img, width, height, err);
-    if (f.size() >= 2 && f[0] == '#' && f[1] == '?') return load_hdr(f, img, width, height, err);
-    if (f.size() >= 2 && f[0] == 'P' && f[1] == '5') return load_pgm(f, img, width, height, err);
+    if (f.size() >= 8 && !std::memcmp(f.data(), png_sig, 8)) return load_png(f, img, width, height, comps, err);
+    if (f.size() >= 2 && f[0] == '#' && f[1] == '?') return load_hdr(f, img, width, height, comps, err);
+    if (f.size() >= 2 && f[0] == 'P' && f[1] == '5') return load_pgm(f, img, width, height, comps, err);
     return err = "unsupported image format (PNG, Radiance HDR and binary PGM are read)", false;
 }
 
-bool write_hdr(const std::string &path, const float *img, int width, int height) {
-    if (width <= 0 || height <= 0 || !img) return false;
+bool load_gray(const std::string &path, std::vector<float> &img, int &width, int &height, std::string &err) {
+    return load_image(path, 1, img, width, height, err);
+}
+
+bool write_hdr(const std::string &path, const float *img, int width, int height, int comps) {
+    if (width <= 0 || height <= 0 || !img || (comps != 1 && comps != 3)) return false;
     std::vector<uint8_t> out;
     const std::string head = "#?RADIANCE\n# Written by lpaici\nFORMAT=32-bit_rle_rgbe\n"
                              "EXPOSURE=          1.0000000000000\n\n-Y " +
@@ -375,18 +408,18 @@ bool write_hdr(const std::string &path, const float *img, int width, int height)
     out.insert(out.end(), head.begin(), head.end());
     std::vector<uint8_t> comp(static_cast<size_t>(width) * 4);
     for (int y = 0; y < height; y++) {
-        const float *row = img + static_cast<size_t>(y) * width;
+        const float *row = img + static_cast<size_t>(y) * width * comps;
         if (width < 8 || width >= 32768) {
             for (int x = 0; x < width; x++) {
                 uint8_t p[4];
-                gray_rgbe(row[x], p);
+                pixel_rgbe(row + static_cast<size_t>(x) * comps, comps, p);
                 out.insert(out.end(), p, p + 4);
             }
             continue;
         }
         for (int x = 0; x < width; x++) {
             uint8_t p[4];
-            gray_rgbe(row[x], p);
+            pixel_rgbe(row + static_cast<size_t>(x) * comps, comps, p);
             for (int k = 0; k < 4; k++) comp[static_cast<size_t>(k) * width + x] = p[k];
         }
         out.push_back(2);
@@ -426,6 +459,27 @@ __attribute__((visibility("default"))) void lpaici_io_free(void *p) { std::free(
 // Writes a one-channel float image as Radiance .hdr.  Returns 0 or -1.
 __attribute__((visibility("default"))) int lpaici_io_write_hdr(const char *path, const float *img, int width,
                                                                int height) {
-    return path && lpaici_cli::write_hdr(path, img, width, height) ? 0 : -1;
+    return path && lpaici_cli::write_hdr(path, img, width, height, 1) ? 0 : -1;
+}
+
+// Loads an RGB float image (width x height x 3, interleaved), as stbi_loadf(path, .., 3) returns it;
+// *out is malloc'd (free with lpaici_io_free).  Returns 0 or -1.
+__attribute__((visibility("default"))) int lpaici_io_load_rgb(const char *path, float **out, int *width, int *height) {
+    std::vector<float> img;
+    std::string err;
+    int w = 0, h = 0;
+    if (!path || !out || !lpaici_cli::load_image(path, 3, img, w, h, err)) return -1;
+    *out = static_cast<float *>(std::malloc(sizeof(float) * img.size()));
+    if (!*out) return -1;
+    std::memcpy(*out, img.data(), sizeof(float) * img.size());
+    *width = w;
+    *height = h;
+    return 0;
+}
+
+// Writes an interleaved RGB float image as Radiance .hdr.  Returns 0 or -1.
+__attribute__((visibility("default"))) int lpaici_io_write_hdr_rgb(const char *path, const float *img, int width,
+                                                                   int height) {
+    return path && lpaici_cli::write_hdr(path, img, width, height, 3) ? 0 : -1;
 }
 }

@@ -18,7 +18,12 @@ namespace lpaici_cli {
 
 // Returns false and sets err on failure.
 bool load_gray(const std::string &path, std::vector<float> &img, int &width, int &height, std::string &err);
-bool write_hdr(const std::string &path, const float *img, int width, int height);
+// comps 1: as load_gray; comps 3: interleaved R, G, B as stbi_loadf(path, .., 3) returns them (gray
+// files replicated, alpha dropped, 16-bit samples' high bytes, HDR mantissas times 2^(E - 136)).
+bool load_image(const std::string &path, int comps, std::vector<float> &img, int &width, int &height,
+                std::string &err);
+// comps 1 (gray, stored R = G = B) or 3 (interleaved RGB), RGBE as stbi_write_hdr encodes it.
+bool write_hdr(const std::string &path, const float *img, int width, int height, int comps = 1);
 
 // The 256 values of stb's 8-bit to float conversion (pow(v/255, 2.2)).
 const float *ldr_to_float_table();

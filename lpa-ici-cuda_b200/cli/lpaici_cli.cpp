@@ -4,7 +4,11 @@
 // reference's fastest GPU executable (main of src/v4_1_lpa_ici_2D_sparse_shared.cu:365-530),
 // computed by the B200 library through its C ABI.
 //
-//   lpaici [-i image] [-k kernels] [-o output.hdr] [-s sigma(0-255)] [-g gamma] [--seed n] [-h]
+//   lpaici [-i image] [-k kernels] [-o output.hdr] [-s sigma(0-255)] [-g gamma] [--seed n] [--color] [-h]
+//
+// --color (not in the reference, which converts every image to gray) keeps the image's R, G and B
+// channels, adds noise to all of them and denoises each channel on its own; its files are
+// color_image.hdr, color_image_noisy.hdr and the RGB -o file, its PSNR lines cover all channels.
 //
 // Errors print a message and exit with status 1, as the reference does; nothing here calls exit()
 // from inside the library.
@@ -28,6 +32,7 @@ struct Config {
     float sigma_noise = 20.0f / 255.0f;
     unsigned int noise_seed = 20250910u;
     float ici_gamma = 2.0f;
+    bool color = false;
 };
 
 std::string dir_of(const std::string &path) {
@@ -44,6 +49,7 @@ void usage(const char *prog) {
               << "  -s, --sigma <value>    noise standard deviation on the 0-255 scale (default 20)\n"
               << "  -g, --gamma <value>    ICI threshold (default " << d.ici_gamma << ")\n"
               << "      --seed <value>     noise seed (default " << d.noise_seed << ")\n"
+              << "      --color            denoise the R, G, B channels (default: gray, as the reference)\n"
               << "  -h, --help             show this message\n";
 }
 
@@ -66,6 +72,10 @@ Config parse(int argc, char **argv) {
         if (opt == "-h" || opt == "--help") {
             usage(argv[0]);
             std::exit(EXIT_SUCCESS);
+        }
+        if (opt == "--color") {
+            cfg.color = true;
+            continue;
         }
         if (i + 1 >= argc) fail(argv[0], "unknown option or missing value for '" + opt + "'");
         const char *val = argv[++i];
@@ -109,24 +119,25 @@ int main(int argc, char **argv) {
     std::vector<float> clean;
     int width = 0, height = 0;
     std::string err;
-    if (!lpaici_cli::load_gray(cfg.image_file, clean, width, height, err)) {
+    const int channels = cfg.color ? 3 : 1;
+    if (!lpaici_cli::load_image(cfg.image_file, channels, clean, width, height, err)) {
         std::cerr << "Error in loading the image " << cfg.image_file << "\n";
         return 1;
     }
-    const int channels = 1;
     std::cout << "Loaded image with a width of " << width << " px, a height of " << height
               << " px and (imported) " << channels << " channels\n";
 
-    const std::string gray_file = dir_of(cfg.output_file) + "gray_image.hdr";
-    std::cout << "Saving gray image as " << gray_file << "\n";
-    lpaici_cli::write_hdr(gray_file, clean.data(), width, height);
+    const std::string kind = cfg.color ? "color" : "gray";
+    const std::string gray_file = dir_of(cfg.output_file) + kind + "_image.hdr";
+    std::cout << "Saving " << kind << " image as " << gray_file << "\n";
+    lpaici_cli::write_hdr(gray_file, clean.data(), width, height, channels);
 
-    const long n = static_cast<long>(width) * height;
+    const long n = static_cast<long>(width) * height * channels;
     std::vector<float> noisy(n);
     lpaici_add_noise(clean.data(), noisy.data(), n, cfg.sigma_noise, cfg.noise_seed);
-    const std::string noisy_file = dir_of(cfg.output_file) + "gray_image_noisy.hdr";
-    std::cout << "Saving noisy gray image as " << noisy_file << "\n";
-    lpaici_cli::write_hdr(noisy_file, noisy.data(), width, height);
+    const std::string noisy_file = dir_of(cfg.output_file) + kind + "_image_noisy.hdr";
+    std::cout << "Saving noisy " << kind << " image as " << noisy_file << "\n";
+    lpaici_cli::write_hdr(noisy_file, noisy.data(), width, height, channels);
 
     const double psnr_noisy = lpaici_psnr(clean.data(), noisy.data(), n);
     std::cout << "Calculated PSNR of host_img_gray_noisy: " << psnr_noisy << "\n";
@@ -166,7 +177,7 @@ int main(int argc, char **argv) {
     const double psnr_denoised = lpaici_psnr(clean.data(), denoised.data(), n);
     std::cout << "Calculated PSNR of img_denoised: " << psnr_denoised << "\n";
     std::cout << "Saving denoised image as " << cfg.output_file.c_str() << "\n";
-    lpaici_cli::write_hdr(cfg.output_file, denoised.data(), width, height);
+    lpaici_cli::write_hdr(cfg.output_file, denoised.data(), width, height, channels);
 
     lpaici_kernelset_destroy(ks);
     return 0;

@@ -90,4 +90,15 @@ unsigned char *ref_stbi_load_u8(const char *path, int *W, int *H) {
 // stbi_write_hdr of a one-channel float image.
 int ref_stbi_write_hdr(const char *path, int W, int H, const float *data) { return stbi_write_hdr(path, W, H, 1, data); }
 
+// stbi_loadf(path, ..., 3): interleaved RGB float image.  Free with ref_stbi_free.
+float *ref_stbi_loadf_rgb(const char *path, int *W, int *H) {
+    int c = 0;
+    return stbi_loadf(path, W, H, &c, 3);
+}
+
+// stbi_write_hdr of an interleaved RGB float image.
+int ref_stbi_write_hdr_rgb(const char *path, int W, int H, const float *data) {
+    return stbi_write_hdr(path, W, H, 3, data);
+}
+
 }  // extern "C"

@@ -206,6 +206,10 @@ def ref_lib(name: str = "v1_0") -> C.CDLL:
             lib.ref_stbi_load_u8.restype = C.POINTER(C.c_ubyte)
             lib.ref_stbi_write_hdr.argtypes = [C.c_char_p, C.c_int, C.c_int, _f32p]
             lib.ref_stbi_write_hdr.restype = C.c_int
+            lib.ref_stbi_loadf_rgb.argtypes = [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+            lib.ref_stbi_loadf_rgb.restype = C.POINTER(C.c_float)
+            lib.ref_stbi_write_hdr_rgb.argtypes = [C.c_char_p, C.c_int, C.c_int, _f32p]
+            lib.ref_stbi_write_hdr_rgb.restype = C.c_int
         else:
             lib.ref_pack_runs.argtypes = [_f32p, _i32p, _i32p, _i32p, C.c_int, _f32p, _i32p, _i32p, _i32p, _i32p,
                                           _i32p, _i32p, C.POINTER(C.c_int)]
@@ -294,3 +298,21 @@ def ref_pack_runs(k: DenseKernels):
     nr = lib.ref_pack_runs(k.w, k.off, k.rows, k.cols, k.nk, weights, rr, rc, rl, kfr, knr, kfw, C.byref(nw))
     return dict(weights=weights[: nw.value], run_row=rr[:nr], run_col=rc[:nr], run_len=rl[:nr],
                 k_first_run=kfr, k_num_runs=knr, k_first_weight=kfw)
+
+
+def ref_stbi_loadf_rgb(path: str) -> np.ndarray:
+    """stbi_loadf(path, .., 3) of the reference's vendored stb_image: H x W x 3."""
+    lib = ref_lib("v1_0")
+    W, H = C.c_int(), C.c_int()
+    p = lib.ref_stbi_loadf_rgb(path.encode(), C.byref(W), C.byref(H))
+    if not p:
+        raise IOError(path)
+    img = np.ctypeslib.as_array(p, shape=(H.value, W.value, 3)).copy()
+    lib.ref_stbi_free(C.cast(p, C.c_void_p))
+    return img
+
+
+def ref_stbi_write_hdr_rgb(path: str, img: np.ndarray) -> None:
+    H, W, _ = img.shape
+    if not ref_lib("v1_0").ref_stbi_write_hdr_rgb(path.encode(), W, H, np.ascontiguousarray(img, np.float32).ravel()):
+        raise IOError(path)

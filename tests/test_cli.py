@@ -27,6 +27,10 @@ IO.lpaici_io_load_gray.argtypes = [C.c_char_p, C.POINTER(C.POINTER(C.c_float)), 
 IO.lpaici_io_free.argtypes = [C.c_void_p]
 IO.lpaici_io_write_hdr.argtypes = [C.c_char_p, np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS"), C.c_int,
                                    C.c_int]
+IO.lpaici_io_load_rgb.argtypes = [C.c_char_p, C.POINTER(C.POINTER(C.c_float)), C.POINTER(C.c_int),
+                                  C.POINTER(C.c_int)]
+IO.lpaici_io_write_hdr_rgb.argtypes = [C.c_char_p, np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS"), C.c_int,
+                                       C.c_int]
 needs_ref = pytest.mark.skipif(not ob.ref_available("v1_0"), reason="reference not built in-process")
 
 
@@ -35,6 +39,15 @@ def io_load(path):
     if IO.lpaici_io_load_gray(path.encode(), C.byref(p), C.byref(w), C.byref(h)) != 0:
         raise ValueError(path)
     a = np.ctypeslib.as_array(p, shape=(h.value * w.value,)).copy().reshape(h.value, w.value)
+    IO.lpaici_io_free(C.cast(p, C.c_void_p))
+    return a
+
+
+def io_load_rgb(path):
+    p, w, h = C.POINTER(C.c_float)(), C.c_int(), C.c_int()
+    if IO.lpaici_io_load_rgb(path.encode(), C.byref(p), C.byref(w), C.byref(h)) != 0:
+        raise ValueError(path)
+    a = np.ctypeslib.as_array(p, shape=(h.value * w.value * 3,)).copy().reshape(h.value, w.value, 3)
     IO.lpaici_io_free(C.cast(p, C.c_void_p))
     return a
 
@@ -179,6 +192,45 @@ def test_png_decoding_matches_stb(tmp_path, ctype, depth, interlace):
     assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
 
 
+@needs_ref
+@pytest.mark.parametrize("ctype,depth", PNG_CASES)
+def test_png_rgb_decoding_matches_stb(tmp_path, ctype, depth):
+    """The colour mode's loader against stbi_loadf(path, .., 3) on every PNG type."""
+    rng = np.random.default_rng(ctype * 101 + depth)
+    H, W = 11, 19
+    ch = {0: 1, 2: 3, 3: 1, 4: 2, 6: 4}[ctype]
+    pal = None
+    if ctype == 3:
+        n = min(256, 1 << depth)
+        pal = rng.integers(0, 256, (n, 3)).astype(np.uint8)
+        arr = rng.integers(0, n, (H, W, 1))
+    else:
+        arr = rng.integers(0, (1 << depth), (H, W, ch))
+    p = str(tmp_path / "c.png")
+    make_png(p, arr, ctype, depth, pal, False)
+    ref = ob.ref_stbi_loadf_rgb(p)
+    got = io_load_rgb(p)
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+
+
+@needs_ref
+@pytest.mark.parametrize("W,H", [(64, 40), (5, 7), (300, 2)])
+def test_hdr_rgb_roundtrip_with_stb(tmp_path, W, H):
+    """RGB .hdr writing and reading: same pixel bytes as stbi_write_hdr(.., 3), both loaders agree."""
+    rng = np.random.default_rng(W + H)
+    img = rng.uniform(0.0, 2.0, (H, W, 3)).astype(np.float32)
+    img[0, 0] = 0.0
+    img[-1, -1, 1] = 1e-35
+    ours, theirs = str(tmp_path / "ours.hdr"), str(tmp_path / "stb.hdr")
+    assert IO.lpaici_io_write_hdr_rgb(ours.encode(), np.ascontiguousarray(img), W, H) == 0
+    ob.ref_stbi_write_hdr_rgb(theirs, img)
+    a, b = open(ours, "rb").read(), open(theirs, "rb").read()
+    assert a[a.index(b"-Y"):] == b[b.index(b"-Y"):]
+    assert np.array_equal(io_load_rgb(theirs).view(np.uint32), ob.ref_stbi_loadf_rgb(theirs).view(np.uint32))
+    # the gray loader of an RGB file averages the channels as stbi_loadf(.., 1) does
+    assert np.array_equal(io_load(theirs).view(np.uint32), ob.ref_stbi_loadf(theirs).view(np.uint32))
+
+
 def test_barbara_png_to_float():
     """data/barbara.png decoded and converted like stb (hash of the reference's float image)."""
     meta = json.load(open(os.path.join(GOLDEN, "barbara.json")))
@@ -238,3 +290,35 @@ def test_cli_barbara_end_to_end(tmp_path):
     den = lpaici.denoise_host(ks, noisy, float(np.float32(20.0) / np.float32(255.0)), 2.0)
     assert hashlib.sha256(den.tobytes()).hexdigest() == meta["denoised_sha256"]
     assert np.array_equal(io_load(str(out)).view(np.uint32), rgbe_quantize(den).view(np.uint32))
+
+
+@pytest.mark.gpu
+def test_cli_color_end_to_end(tmp_path):
+    """--color: R, G, B loaded as stb does, noise over all channels, every channel denoised on its own;
+    the RGB output file holds exactly the library's interleaved-channel result."""
+    import torch
+
+    rng = np.random.default_rng(5)
+    H, W = 72, 96
+    rgb = np.stack([np.round(lpaici.synth_image(W, H, 60 + c, rgbe=False) * 255) for c in range(3)], axis=2)
+    rgb = np.clip(rgb + rng.integers(-3, 4, rgb.shape), 0, 255).astype(np.int64)
+    img = tmp_path / "c.png"
+    make_png(str(img), rgb, 2, 8)
+    out = tmp_path / "den.hdr"
+    r = run_cli("-i", str(img), "-k", kernel_file(SYM), "-o", str(out), "-s", "25", "--color")
+    assert r.returncode == 0, r.stderr
+    lines = r.stdout.splitlines()
+    assert any("and (imported) 3 channels" in ln for ln in lines)
+    for f in ("color_image.hdr", "color_image_noisy.hdr", "den.hdr"):
+        assert (tmp_path / f).exists()
+    sigma = float(np.float32(25.0) / np.float32(255.0))
+    clean = io_load_rgb(str(img))
+    noisy = lpaici.add_noise(clean.reshape(-1), sigma, 20250910).reshape(H, W, 3)
+    ks = lpaici.KernelSet.load(kernel_file(SYM))
+    den = lpaici.forward_channels(ks, torch.from_numpy(noisy).cuda(), sigma, 2.0).cpu().numpy()
+    mine = tmp_path / "mine.hdr"
+    assert IO.lpaici_io_write_hdr_rgb(str(mine).encode(), np.ascontiguousarray(den), W, H) == 0
+    a, b = open(out, "rb").read(), open(mine, "rb").read()
+    assert a[a.index(b"-Y"):] == b[b.index(b"-Y"):]
+    want = f"Calculated PSNR of img_denoised: {lpaici.psnr(clean, den):.6g}"
+    assert want in lines, (want, [ln for ln in lines if "PSNR" in ln])
