@@ -200,6 +200,21 @@ int lpaici_backward(const lpaici_kernelset *ks, const float *d_noisy, int noisy_
                     int gout_pitch, float *d_grad_in, int gin_pitch, int width, int height, float sigma,
                     float gamma, lpaici_stream_t stream);
 
+/* Kept state, for callers that run the forward and then its adjoint (a training step) and can hold
+ * D + 4 bytes per pixel: lpaici_forward_state is lpaici_forward (same output, bit for bit) that also
+ * stores the selected scales and 1/den in caller-owned device memory d_state of
+ * lpaici_adjoint_state_bytes(ks, width, height) bytes; lpaici_backward_state then runs the adjoint's
+ * gather only (no selection pass), with the same sigma, and gives lpaici_backward's gradient bit for
+ * bit.  lpaici_backward itself keeps nothing and recomputes the selection.  No counterpart in the
+ * reference. */
+size_t lpaici_adjoint_state_bytes(const lpaici_kernelset *ks, int width, int height);
+int lpaici_forward_state(const lpaici_kernelset *ks, const float *d_noisy, int noisy_pitch, float *d_denoised,
+                         int out_pitch, int width, int height, float sigma, float gamma, void *d_state,
+                         lpaici_stream_t stream);
+int lpaici_backward_state(const lpaici_kernelset *ks, const void *d_state, const float *d_grad_out, int gout_pitch,
+                          float *d_grad_in, int gin_pitch, int width, int height, float sigma,
+                          lpaici_stream_t stream);
+
 /* One image of a batched adjoint: noisy input, cotangent g and the gradient's buffer (device pointers,
  * pitches in floats), with the image's sigma and gamma. */
 typedef struct {

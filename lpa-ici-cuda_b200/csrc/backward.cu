@@ -277,17 +277,17 @@ long gather_tiles(int width, int height, int *tiles_x) {
 
 }  // namespace
 
+int gather_pass(const lpaici_kernelset *ks, const int *adj_blob, const uint8_t *smap, const float *rden,
+                const float *d_grad_out, int gout_pitch, float *d_grad_in, int gin_pitch, int width, int height,
+                float sigma, cudaStream_t stream);
+
 // The two passes over caller-provided storage (lpaici_backward, lpaici_backward_noalloc).
 int adjoint_passes(const lpaici_kernelset *ks, const int *blob, const int *adj_blob, uint8_t *smap, float *rden,
                    const float *d_noisy, int noisy_pitch, const float *d_grad_out, int gout_pitch, float *d_grad_in,
                    int gin_pitch, int width, int height, float sigma, float gamma, cudaStream_t stream) {
-    GatherArgs ga{};
-    size_t smem = 0;
-    int rc = gather_setup(ks, adj_blob, &ga, &smem);
-    if (rc != LPAICI_OK) return rc;
     int tiles_x = 0;
-    const long tiles = gather_tiles(width, height, &tiles_x);
-    if (tiles > 0x7fffffffL) return set_error(LPAICI_ERR_UNSUPPORTED, "image too large: %d x %d", width, height);
+    if (gather_tiles(width, height, &tiles_x) > 0x7fffffffL)
+        return set_error(LPAICI_ERR_UNSUPPORTED, "image too large: %d x %d", width, height);
 
     // A. selection
     ImageArgs img{};
@@ -304,10 +304,27 @@ int adjoint_passes(const lpaici_kernelset *ks, const int *blob, const int *adj_b
     KernelTables tab;
     fill_tables(ks, nullptr, sigma, gamma, &tab);
     tab.blob = blob;
-    rc = launch_forward(ks, img, tab, default_config(ks), stream);
+    const int rc = launch_forward(ks, img, tab, default_config(ks), stream);
     if (rc != LPAICI_OK) return rc;
 
     // B. gather
+    return gather_pass(ks, adj_blob, smap, rden, d_grad_out, gout_pitch, d_grad_in, gin_pitch, width, height, sigma,
+                       stream);
+}
+
+// Pass B alone, from the s* planes and 1/den of the image (pass A's outputs or a kept state).
+int gather_pass(const lpaici_kernelset *ks, const int *adj_blob, const uint8_t *smap, const float *rden,
+                const float *d_grad_out, int gout_pitch, float *d_grad_in, int gin_pitch, int width, int height,
+                float sigma, cudaStream_t stream) {
+    GatherArgs ga{};
+    size_t smem = 0;
+    int rc = gather_setup(ks, adj_blob, &ga, &smem);
+    if (rc != LPAICI_OK) return rc;
+    int tiles_x = 0;
+    const long tiles = gather_tiles(width, height, &tiles_x);
+    if (tiles > 0x7fffffffL) return set_error(LPAICI_ERR_UNSUPPORTED, "image too large: %d x %d", width, height);
+    KernelTables tab;
+    fill_tables(ks, nullptr, sigma, 1.0f, &tab);
     ga.single = GatherImage{d_grad_out, smap, rden, d_grad_in, nullptr, gout_pitch, gin_pitch, width, height, tiles_x, 0};
     for (int k = 0; k < ks->D * ks->S; k++) ga.rvar[k] = 1.0f / tab.var[k];
     lpaici_adjoint_gather_kernel<<<static_cast<unsigned>(tiles), kGatherThreads, smem, stream>>>(ga);
@@ -601,4 +618,73 @@ extern "C" int lpaici_backward_batch_destroy(lpaici_backward_batch *b) {
         if (cur >= 0) cudaSetDevice(cur);
     }
     return LPAICI_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Kept state: the forward stores what its adjoint needs, the adjoint runs the gather only.
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+size_t state_smap_bytes(const lpaici_kernelset *ks, int width, int height) {
+    return (static_cast<size_t>(ks->D) * width * height + 255) & ~size_t(255);
+}
+
+int state_args(const lpaici_kernelset *ks, int width, int height, float sigma, const char *who) {
+    if (!ks) return set_error(LPAICI_ERR_INVALID_ARG, "%s: null kernel set", who);
+    if (width <= 0 || height <= 0) return set_error(LPAICI_ERR_INVALID_ARG, "%s: bad size %d x %d", who, width, height);
+    if (!(sigma > 0.0f)) return set_error(LPAICI_ERR_INVALID_ARG, "%s: sigma needs a positive number", who);
+    if (ks->S > 32) return set_error(LPAICI_ERR_UNSUPPORTED, "%s: the adjoint supports at most 32 scales", who);
+    return LPAICI_OK;
+}
+
+}  // namespace
+
+extern "C" size_t lpaici_adjoint_state_bytes(const lpaici_kernelset *ks, int width, int height) {
+    if (!ks || width <= 0 || height <= 0) return 0;
+    return state_smap_bytes(ks, width, height) + sizeof(float) * static_cast<size_t>(width) * height;
+}
+
+extern "C" int lpaici_forward_state(const lpaici_kernelset *ks, const float *d_noisy, int noisy_pitch,
+                                    float *d_denoised, int out_pitch, int width, int height, float sigma, float gamma,
+                                    void *d_state, lpaici_stream_t stream_) {
+    int rc = state_args(ks, width, height, sigma, "lpaici_forward_state");
+    if (rc != LPAICI_OK) return rc;
+    if (!d_noisy || !d_denoised || !d_state || noisy_pitch < width || out_pitch < width)
+        return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_forward_state: null pointer or bad pitch");
+    if (!(gamma > 0.0f)) return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_forward_state: gamma needs a positive number");
+    const int *blob = nullptr;
+    rc = device_blob(ks, &blob);
+    if (rc != LPAICI_OK) return rc;
+    ImageArgs img{};
+    img.in = d_noisy;
+    img.out = d_denoised;
+    img.smap = static_cast<uint8_t *>(d_state);
+    img.rden = reinterpret_cast<float *>(static_cast<char *>(d_state) + state_smap_bytes(ks, width, height));
+    img.W = width;
+    img.in_h = height;
+    img.in_pitch = noisy_pitch;
+    img.out_pitch = out_pitch;
+    img.row_begin = 0;
+    img.rows_out = height;
+    KernelTables tab;
+    fill_tables(ks, nullptr, sigma, gamma, &tab);
+    tab.blob = blob;
+    return launch_forward(ks, img, tab, default_config(ks), reinterpret_cast<cudaStream_t>(stream_));
+}
+
+extern "C" int lpaici_backward_state(const lpaici_kernelset *ks, const void *d_state, const float *d_grad_out,
+                                     int gout_pitch, float *d_grad_in, int gin_pitch, int width, int height, float sigma,
+                                     lpaici_stream_t stream_) {
+    int rc = state_args(ks, width, height, sigma, "lpaici_backward_state");
+    if (rc != LPAICI_OK) return rc;
+    if (!d_state || !d_grad_out || !d_grad_in || gout_pitch < width || gin_pitch < width)
+        return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_backward_state: null pointer or bad pitch");
+    const int *adj = nullptr;
+    rc = device_adj_blob(ks, &adj);
+    if (rc != LPAICI_OK) return rc;
+    const uint8_t *smap = static_cast<const uint8_t *>(d_state);
+    const float *rden =
+        reinterpret_cast<const float *>(static_cast<const char *>(d_state) + state_smap_bytes(ks, width, height));
+    return gather_pass(ks, adj, smap, rden, d_grad_out, gout_pitch, d_grad_in, gin_pitch, width, height, sigma,
+                       reinterpret_cast<cudaStream_t>(stream_));
 }

@@ -102,6 +102,9 @@ _SIGS = {
     "lpaici_backward_noalloc": ([_vp, _vp, _i, _vp, _i, _vp, _i, _i, _i, _f, _f, _vp], _i),
     "lpaici_trim_workspace": ([], _i),
     "lpaici_forward_channels": ([_vp, _vp, _i, _vp, _i, _i, _i, _i, _f, _f, _vp], _i),
+    "lpaici_adjoint_state_bytes": ([_vp, _i, _i], C.c_size_t),
+    "lpaici_forward_state": ([_vp, _vp, _i, _vp, _i, _i, _i, _f, _f, _vp, _vp], _i),
+    "lpaici_backward_state": ([_vp, _vp, _vp, _i, _vp, _i, _i, _i, _f, _vp], _i),
     "lpaici_backward_batch_create": ([_vp, C.POINTER(GradImage), _i, C.POINTER(BatchOptions), _vp, C.POINTER(_vp)],
                                      _i),
     "lpaici_backward_batch_run": ([_vp, _vp], _i),
@@ -342,6 +345,45 @@ def forward_channels(ks: KernelSet, noisy, sigma: float, gamma: float, out=None)
                                           _stream(torch))
     _check(rc, "lpaici_forward_channels")
     return out
+
+
+def forward_state(ks: KernelSet, noisy, sigma: float, gamma: float, out=None, state=None):
+    """lpaici_forward_state: (denoised, state), the state (uint8 CUDA tensor, reused when given) holding
+    what backward_state needs."""
+    import torch
+
+    _check_image(noisy, "noisy")
+    H, W = noisy.shape
+    if out is None:
+        out = torch.empty((H, W), dtype=torch.float32, device=noisy.device)
+    _check_image(out, "out")
+    nbytes = int(_lib.lpaici_adjoint_state_bytes(ks.handle, W, H))
+    if state is None:
+        state = torch.empty(nbytes, dtype=torch.uint8, device=noisy.device)
+    elif state.numel() < nbytes or state.dtype != torch.uint8:
+        raise ValueError(f"state: a uint8 tensor of at least {nbytes} bytes")
+    with torch.cuda.device(noisy.device):
+        rc = _lib.lpaici_forward_state(ks.handle, C.c_void_p(noisy.data_ptr()), noisy.stride(0),
+                                       C.c_void_p(out.data_ptr()), out.stride(0), W, H, sigma, gamma,
+                                       C.c_void_p(state.data_ptr()), _stream(torch))
+    _check(rc, "lpaici_forward_state")
+    return out, state
+
+
+def backward_state(ks: KernelSet, state, grad_out, sigma: float, grad_in=None):
+    """lpaici_backward_state: the adjoint from a forward_state state (gather pass only)."""
+    import torch
+
+    _check_image(grad_out, "grad_out")
+    H, W = grad_out.shape
+    if grad_in is None:
+        grad_in = torch.empty((H, W), dtype=torch.float32, device=grad_out.device)
+    with torch.cuda.device(grad_out.device):
+        rc = _lib.lpaici_backward_state(ks.handle, C.c_void_p(state.data_ptr()), C.c_void_p(grad_out.data_ptr()),
+                                        grad_out.stride(0), C.c_void_p(grad_in.data_ptr()), grad_in.stride(0), W, H,
+                                        sigma, _stream(torch))
+    _check(rc, "lpaici_backward_state")
+    return grad_in
 
 
 def backward(ks: KernelSet, noisy, grad_out, sigma: float, gamma: float, grad_in=None):

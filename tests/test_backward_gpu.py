@@ -99,3 +99,20 @@ def test_backward_errors():
     x = torch.zeros((4, 4), device="cuda")
     with pytest.raises(lpaici.LpaIciError):
         lpaici.backward(ks, x, x, -1.0, 2.0)
+
+
+@pytest.mark.parametrize("name,W,H", [(SYM, 257, 131), (GAUSS_M2, 96, 200), (SYM, 1, 1)])
+def test_kept_state_equals_recomputation(name, W, H):
+    """lpaici_forward_state gives lpaici_forward's output and keeps a state from which
+    lpaici_backward_state gives lpaici_backward's gradient, both bit for bit."""
+    import torch
+
+    ks = lpaici.KernelSet.load(kernel_file(name))
+    sigma = SIGMA_20
+    x = torch.from_numpy(lpaici.add_noise(lpaici.synth_image(W, H, 3), sigma, 4)).cuda()
+    g = torch.from_numpy(np.random.default_rng(5).standard_normal((H, W)).astype(np.float32)).cuda()
+    out, state = lpaici.forward_state(ks, x, sigma, 2.0)
+    assert torch.equal(out.view(torch.int32), lpaici.forward(ks, x, sigma, 2.0).view(torch.int32))
+    got = lpaici.backward_state(ks, state, g, sigma)
+    ref = lpaici.backward(ks, x, g, sigma, 2.0)
+    assert torch.equal(got.view(torch.int32), ref.view(torch.int32))
