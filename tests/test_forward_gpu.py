@@ -253,3 +253,22 @@ def test_interleaved_channels_equal_single_channel(channels):
         ref = lpaici.forward(ks, torch.from_numpy(planes[c]).cuda(), SIGMA_20, 2.0).cpu().numpy()
         assert np.array_equal(out[:, :, c].view(np.uint32), ref.view(np.uint32)), c
         assert np.array_equal(host_out[:, :, c].view(np.uint32), ref.view(np.uint32)), c
+
+
+def test_limits_refused(torch):
+    """Kernel sets beyond the kernels' limits are refused with LPAICI_ERR_UNSUPPORTED, not run: more
+    than 16 scales per direction (the sweeps keep a 4-bit scale index), a radius above 127."""
+    x = torch.zeros((16, 16), device="cuda")
+    S = 17
+    ks = lpaici.KernelSet.from_dense(np.ones(S, np.float32), np.arange(S), np.ones(S), np.ones(S), 1, S)
+    with pytest.raises(lpaici.LpaIciError) as e:
+        lpaici.forward(ks, x, 0.1, 2.0)
+    assert e.value.code == lpaici.ERR_UNSUPPORTED and "16" in str(e.value)
+    with pytest.raises(lpaici.LpaIciError) as e:
+        lpaici.Batch(ks, [x], [torch.empty_like(x)], [0.1], [2.0])
+    assert e.value.code == lpaici.ERR_UNSUPPORTED
+    w = np.zeros(257 * 257, np.float32)
+    w[0] = 1.0  # a tap 128 rows and columns from the centre
+    with pytest.raises(lpaici.LpaIciError) as e:
+        lpaici.KernelSet.from_dense(w, [0], [257], [257], 1, 1)
+    assert e.value.code == lpaici.ERR_UNSUPPORTED
