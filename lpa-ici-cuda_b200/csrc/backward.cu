@@ -28,13 +28,19 @@ namespace lpaici {
 namespace {
 
 constexpr int kGatherP = 9;  // outputs per thread (odd: conflict-free scalar shared loads)
-constexpr int kGatherWX = 2, kGatherWY = 8;
-constexpr int kGatherTW = kGatherWX * 4 * kGatherP, kGatherTH = kGatherWY * 8;  // 72 x 64 outputs
+constexpr int kGatherWX = 2;
+constexpr int kGatherTW = kGatherWX * 4 * kGatherP;  // 72 output columns; 8 * WY rows (WY = 8: 64)
 // Two groups of 16 warps cover the same outputs, each with every other run of a kernel; their partial
 // sums are added at the end (1024 threads: twice the warps to hide shared-memory latency).
 constexpr int kGatherGroups = 2;
-constexpr int kGroupThreads = 32 * kGatherWX * kGatherWY;
-constexpr int kGatherThreads = kGatherGroups * kGroupThreads;
+template <int WY>
+struct GatherShape {
+    static constexpr int kTH = 8 * WY;
+    static constexpr int kGroupThreads = 32 * kGatherWX * WY;
+    static constexpr int kThreads = kGatherGroups * kGroupThreads;
+};
+// Tile heights the host can choose (the tallest whose fields and mirrored kernels fit in shared memory).
+constexpr int kGatherWYs[] = {8, 6, 4, 2};
 
 // One image of the gather: pass A's outputs and the caller's buffers.
 struct GatherImage {
@@ -55,6 +61,7 @@ struct GatherArgs {
     const int *blob;       // mirrored kernels (lpaici_kernelset::adj_blob)
     int blob_words, run_word, weight_word;
     int pitch, rows;       // shared-memory field geometry (floats)
+    int th;                // output rows per tile
     float rvar[kMaxKernels];  // 1 / v_k of the one image
     // per kernel: the field rectangle its gathers read, rows [x, y), 4-column groups [z, w)
     int4 rect[kMaxKernels];
@@ -96,8 +103,13 @@ __device__ __forceinline__ void gather_run(float (&acc)[P], const float *__restr
     }
 }
 
-__global__ void __launch_bounds__(kGatherThreads, 1) lpaici_adjoint_gather_kernel(const __grid_constant__ GatherArgs a) {
+template <int WY>
+__global__ void __launch_bounds__(GatherShape<WY>::kThreads, 1)
+    lpaici_adjoint_gather_kernel(const __grid_constant__ GatherArgs a) {
     constexpr int P = kGatherP;
+    constexpr int kGatherTH = GatherShape<WY>::kTH;
+    constexpr int kGroupThreads = GatherShape<WY>::kGroupThreads;
+    constexpr int kGatherThreads = GatherShape<WY>::kThreads;
     extern __shared__ __align__(16) int smem[];
     __shared__ unsigned s_present;
     const int fsize = a.rows * a.pitch;  // a multiple of 4
@@ -221,19 +233,52 @@ namespace {
 
 // The launch-independent part of the gather's arguments: field geometry, mirrored kernels and the
 // per-kernel rectangles; smem receives the dynamic shared memory, checked against the device.
-int gather_setup(const lpaici_kernelset *ks, const int *adj_blob, GatherArgs *ga, size_t *smem) {
+template <int WY>
+const void *gather_fn() {
+    return reinterpret_cast<const void *>(lpaici_adjoint_gather_kernel<WY>);
+}
+const void *gather_fn(int wy) {
+    switch (wy) {
+        case 8: return gather_fn<8>();
+        case 6: return gather_fn<6>();
+        case 4: return gather_fn<4>();
+        default: return gather_fn<2>();
+    }
+}
+
+int gather_launch(const GatherArgs &ga, int wy, unsigned grid, size_t smem, cudaStream_t stream) {
+    switch (wy) {
+        case 8: lpaici_adjoint_gather_kernel<8><<<grid, GatherShape<8>::kThreads, smem, stream>>>(ga); break;
+        case 6: lpaici_adjoint_gather_kernel<6><<<grid, GatherShape<6>::kThreads, smem, stream>>>(ga); break;
+        case 4: lpaici_adjoint_gather_kernel<4><<<grid, GatherShape<4>::kThreads, smem, stream>>>(ga); break;
+        default: lpaici_adjoint_gather_kernel<2><<<grid, GatherShape<2>::kThreads, smem, stream>>>(ga); break;
+    }
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? LPAICI_OK : cuda_error(e, "adjoint gather launch");
+}
+
+// Chooses the tile height (*wy: 8 * wy output rows) and fills the geometry.
+int gather_setup(const lpaici_kernelset *ks, const int *adj_blob, GatherArgs *ga, size_t *smem, int *wy) {
     ga->R = ks->radius;
     ga->pitch = field_pitch(kGatherTW + 2 * ga->R + kGatherP);
-    ga->rows = kGatherTH + 2 * ga->R;
     ga->blob_words = static_cast<int>(ks->adj_blob.size());
-    const size_t fsize = static_cast<size_t>(ga->pitch) * ga->rows;
-    *smem = sizeof(int) * ga->blob_words + 2 * sizeof(float) * fsize + fsize;
     int dev = 0, max_optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    if (*smem > static_cast<size_t>(max_optin))
+    *wy = 0;
+    for (const int w : kGatherWYs) {
+        const size_t fsize = static_cast<size_t>(ga->pitch) * (8 * w + 2 * ga->R);
+        *smem = sizeof(int) * ga->blob_words + 2 * sizeof(float) * fsize + fsize;
+        if (*smem <= static_cast<size_t>(max_optin)) {
+            *wy = w;
+            break;
+        }
+    }
+    if (*wy == 0)
         return set_error(LPAICI_ERR_UNSUPPORTED, "adjoint tile needs %zu B of shared memory, device allows %d", *smem,
                          max_optin);
+    ga->th = 8 * *wy;
+    ga->rows = ga->th + 2 * ga->R;
     ga->D = ks->D;
     ga->S = ks->S;
     ga->blob = adj_blob;
@@ -262,17 +307,17 @@ int gather_setup(const lpaici_kernelset *ks, const int *adj_blob, GatherArgs *ga
             ga->rect[k] = make_int4(0, 0, 0, 0);  // no taps
         } else {
             const int col_end = std::min(ga->pitch, ga->R + kGatherTW + xhi + 1);
-            ga->rect[k] = make_int4(ga->R + ylo, ga->R + kGatherTH + yhi, (ga->R + xlo) >> 2, (col_end + 3) >> 2);
+            ga->rect[k] = make_int4(ga->R + ylo, ga->R + ga->th + yhi, (ga->R + xlo) >> 2, (col_end + 3) >> 2);
         }
     }
-    cudaError_t e = cudaFuncSetAttribute(lpaici_adjoint_gather_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(gather_fn(*wy), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(*smem));
     return e == cudaSuccess ? LPAICI_OK : cuda_error(e, "adjoint gather attributes");
 }
 
-long gather_tiles(int width, int height, int *tiles_x) {
+long gather_tiles(int width, int height, int th, int *tiles_x) {
     *tiles_x = (width + kGatherTW - 1) / kGatherTW;
-    return static_cast<long>(*tiles_x) * ((height + kGatherTH - 1) / kGatherTH);
+    return static_cast<long>(*tiles_x) * ((height + th - 1) / th);
 }
 
 }  // namespace
@@ -286,7 +331,7 @@ int adjoint_passes(const lpaici_kernelset *ks, const int *blob, const int *adj_b
                    const float *d_noisy, int noisy_pitch, const float *d_grad_out, int gout_pitch, float *d_grad_in,
                    int gin_pitch, int width, int height, float sigma, float gamma, cudaStream_t stream) {
     int tiles_x = 0;
-    if (gather_tiles(width, height, &tiles_x) > 0x7fffffffL)
+    if (gather_tiles(width, height, 16, &tiles_x) > 0x7fffffffL)  // the shortest tile the gather may use
         return set_error(LPAICI_ERR_UNSUPPORTED, "image too large: %d x %d", width, height);
 
     // A. selection
@@ -318,18 +363,17 @@ int gather_pass(const lpaici_kernelset *ks, const int *adj_blob, const uint8_t *
                 float sigma, cudaStream_t stream) {
     GatherArgs ga{};
     size_t smem = 0;
-    int rc = gather_setup(ks, adj_blob, &ga, &smem);
+    int wy = 0;
+    int rc = gather_setup(ks, adj_blob, &ga, &smem, &wy);
     if (rc != LPAICI_OK) return rc;
     int tiles_x = 0;
-    const long tiles = gather_tiles(width, height, &tiles_x);
+    const long tiles = gather_tiles(width, height, ga.th, &tiles_x);
     if (tiles > 0x7fffffffL) return set_error(LPAICI_ERR_UNSUPPORTED, "image too large: %d x %d", width, height);
     KernelTables tab;
     fill_tables(ks, nullptr, sigma, 1.0f, &tab);
     ga.single = GatherImage{d_grad_out, smap, rden, d_grad_in, nullptr, gout_pitch, gin_pitch, width, height, tiles_x, 0};
     for (int k = 0; k < ks->D * ks->S; k++) ga.rvar[k] = 1.0f / tab.var[k];
-    lpaici_adjoint_gather_kernel<<<static_cast<unsigned>(tiles), kGatherThreads, smem, stream>>>(ga);
-    const cudaError_t e = cudaGetLastError();
-    return e == cudaSuccess ? LPAICI_OK : cuda_error(e, "adjoint gather launch");
+    return gather_launch(ga, wy, static_cast<unsigned>(tiles), smem, stream);
 }
 
 namespace {
@@ -437,6 +481,7 @@ struct lpaici_backward_batch {
     void *dev_mem = nullptr;         // s* planes | 1/den maps | GatherImage[n] | 1/v tables | items
     GatherArgs ga{};
     size_t smem = 0;
+    int wy = 0;
     unsigned grid = 0;
     bool use_graph = false;
     cudaGraph_t graph = nullptr;
@@ -448,9 +493,7 @@ namespace {
 int backward_batch_enqueue(lpaici_backward_batch *b, cudaStream_t stream) {
     int rc = batch_plan_enqueue(b->select, stream);
     if (rc != LPAICI_OK) return rc;
-    lpaici_adjoint_gather_kernel<<<b->grid, kGatherThreads, b->smem, stream>>>(b->ga);
-    const cudaError_t e = cudaGetLastError();
-    return e == cudaSuccess ? LPAICI_OK : cuda_error(e, "adjoint gather launch");
+    return gather_launch(b->ga, b->wy, b->grid, b->smem, stream);
 }
 
 void backward_batch_free(lpaici_backward_batch *b) {
@@ -488,7 +531,7 @@ extern "C" int lpaici_backward_batch_create(const lpaici_kernelset *ks, const lp
     if (rc != LPAICI_OK) return rc;
     auto *b = new lpaici_backward_batch();
     cudaGetDevice(&b->device);
-    rc = gather_setup(ks, adj, &b->ga, &b->smem);
+    rc = gather_setup(ks, adj, &b->ga, &b->smem, &b->wy);
     if (rc != LPAICI_OK) {
         backward_batch_free(b);
         return rc;
@@ -506,7 +549,7 @@ extern "C" int lpaici_backward_batch_create(const lpaici_kernelset *ks, const lp
         off = align256(off + static_cast<size_t>(ks->D) * npx);
         rden_off[i] = off;
         off = align256(off + sizeof(float) * npx);
-        total_tiles += gather_tiles(images[i].width, images[i].height, &tiles_x[i]);
+        total_tiles += gather_tiles(images[i].width, images[i].height, b->ga.th, &tiles_x[i]);
     }
     if (total_tiles > 0x7fffffffL) {
         backward_batch_free(b);
@@ -541,7 +584,7 @@ extern "C" int lpaici_backward_batch_create(const lpaici_kernelset *ks, const lp
                               reinterpret_cast<const float *>(base + rvar_off) + static_cast<size_t>(i) * nk,
                               im.gout_pitch, im.gin_pitch, im.width, im.height, tiles_x[i], 0};
         int tx = 0;
-        const long t = gather_tiles(im.width, im.height, &tx);
+        const long t = gather_tiles(im.width, im.height, b->ga.th, &tx);
         for (long j = 0; j < t; j++) items.push_back(make_int2(i, static_cast<int>(j)));
         specs[i] = BatchSpec{im.noisy, nullptr, smap, rden, im.width, im.height, im.noisy_pitch, im.width, im.sigma,
                              im.gamma};
