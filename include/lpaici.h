@@ -66,7 +66,8 @@ typedef struct {
  * build_sparse_kernels (src/v4_1_lpa_ici_2D_sparse_shared.cu:826-877) + the constant-memory
  * upload and its capacity checks (src/v4_1_lpa_ici_2D_sparse_shared.cu:1175-1214).
  * Errors: LPAICI_ERR_FILE (cannot open), LPAICI_ERR_KERNEL_FORMAT (bad header, size or weights,
- * or a kernel smaller than direction 0's at its scale), LPAICI_ERR_UNSUPPORTED (radius > 127). */
+ * or a kernel smaller than direction 0's at its scale), LPAICI_ERR_UNSUPPORTED (radius > 127; the
+ * launches refuse radii whose halo'd tile does not fit in shared memory, about 48-60). */
 int lpaici_kernelset_load(const char *path, lpaici_kernelset **out);
 
 /* Builds a kernel set from the loader's dense arrays (weights, offsets, rows, cols: D*S kernels,
