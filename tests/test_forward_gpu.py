@@ -272,3 +272,11 @@ def test_limits_refused(torch):
     with pytest.raises(lpaici.LpaIciError) as e:
         lpaici.KernelSet.from_dense(w, [0], [257], [257], 1, 1)
     assert e.value.code == lpaici.ERR_UNSUPPORTED
+    # radius 70: loads, but its halo'd tile fits no shared-memory budget: the launches refuse it
+    w = np.zeros(141 * 141, np.float32)
+    w[0] = w[-1] = 0.5
+    wide = lpaici.KernelSet.from_dense(w, [0], [141], [141], 1, 1)
+    for call in (lambda: lpaici.forward(wide, x, 0.1, 2.0), lambda: lpaici.backward(wide, x, x, 0.1, 2.0)):
+        with pytest.raises(lpaici.LpaIciError) as e:
+            call()
+        assert e.value.code == lpaici.ERR_UNSUPPORTED and "shared memory" in str(e.value)
