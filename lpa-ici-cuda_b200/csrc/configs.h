@@ -2,7 +2,7 @@
 // down WY, column pairs per thread Q (4 or 8).  A warp covers 16 rows x 4Q columns (2Q pixels per
 // thread), so a CTA covers (4Q*WX) x (16*WY) pixels with 32*WX*WY threads.  The autotuner picks among
 // these per kernel set and device; configurations whose shared memory does not fit a kernel set are
-// skipped.  The adjoint runs the Q = 4 configurations only.
+// skipped.  The adjoint's selection pass runs the configuration the forward uses.
 #pragma once
 
 // X(index, WX, WY, Q)
