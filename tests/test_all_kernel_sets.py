@@ -11,10 +11,9 @@ import pytest
 
 import lpaici
 import oracle_bind as ob
-from conftest import GOLDEN
+from conftest import GOLDEN, REFERENCE_KERNELS
 
 TAPS = sorted(glob.glob(os.path.join(GOLDEN, "kernels", "taps", "*.taps")))
-REFERENCE_KERNELS = "/root/reference/kernels"
 
 
 def _dense(ks):
