@@ -349,7 +349,7 @@ int adjoint_passes(const lpaici_kernelset *ks, const int *blob, const int *adj_b
     KernelTables tab;
     fill_tables(ks, nullptr, sigma, gamma, &tab);
     tab.blob = blob;
-    const int rc = launch_forward(ks, img, tab, default_config(ks), stream);
+    const int rc = launch_forward(ks, img, tab, config_for(ks, width, height), stream);
     if (rc != LPAICI_OK) return rc;
 
     // B. gather
@@ -712,7 +712,7 @@ extern "C" int lpaici_forward_state(const lpaici_kernelset *ks, const float *d_n
     KernelTables tab;
     fill_tables(ks, nullptr, sigma, gamma, &tab);
     tab.blob = blob;
-    return launch_forward(ks, img, tab, default_config(ks), reinterpret_cast<cudaStream_t>(stream_));
+    return launch_forward(ks, img, tab, config_for(ks, width, height), reinterpret_cast<cudaStream_t>(stream_));
 }
 
 extern "C" int lpaici_backward_state(const lpaici_kernelset *ks, const void *d_state, const float *d_grad_out,

@@ -4,6 +4,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "configs.h"
 #include "internal.h"
@@ -20,10 +21,70 @@ int default_config(const lpaici_kernelset *ks) {
             return ks->tuned_config[dev];
     }
     cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    for (int c = 0; c < LPAICI_NUM_TILE_CONFIGS; c++)
+    static const int order[] = LPAICI_TILE_PREFERENCE;
+    static_assert(sizeof(order) / sizeof(order[0]) == LPAICI_NUM_TILE_CONFIGS, "one preference per configuration");
+    for (const int c : order)
         if (config_smem(c, ks->layout.total_words, ks->D * ks->S, ks->radius) <= static_cast<size_t>(max_optin))
             return c;
     return LPAICI_DEFAULT_TILE_CONFIG;  // nothing fits: the launch reports LPAICI_ERR_UNSUPPORTED
+}
+
+// ms one B200 SM (1,965 MHz) spends on one tile of each configuration, measured on the 4096^2
+// benchmark image with the 16x7 symmetric kernels (launch time / waves): the estimate for kernel sets
+// that were not tuned.
+static const float kTileMs[LPAICI_NUM_TILE_CONFIGS] = {0.349f, 0.350f, 0.357f, 0.426f, 0.427f, 0.442f,
+                                                0.261f, 0.412f, 0.412f, 0.485f, 0.479f};
+
+// CTAs per SM of configuration c for ks on device dev (cached; 0 when it does not fit).
+static int cached_bps(const lpaici_kernelset *ks, int dev, int c, int max_optin) {
+    {
+        std::lock_guard<std::mutex> lock(ks->mu);
+        if (dev < static_cast<int>(ks->blocks_per_sm.size()) && !ks->blocks_per_sm[dev].empty() &&
+            ks->blocks_per_sm[dev][c] >= 0)
+            return ks->blocks_per_sm[dev][c];
+    }
+    const size_t smem = config_smem(c, ks->layout.total_words, ks->D * ks->S, ks->radius);
+    const int n = smem <= static_cast<size_t>(max_optin) ? config_blocks_per_sm(c, smem) : 0;
+    std::lock_guard<std::mutex> lock(ks->mu);
+    if (static_cast<int>(ks->blocks_per_sm.size()) <= dev) ks->blocks_per_sm.resize(dev + 1);
+    if (ks->blocks_per_sm[dev].empty()) ks->blocks_per_sm[dev].assign(LPAICI_NUM_TILE_CONFIGS, -1);
+    ks->blocks_per_sm[dev][c] = n;
+    return n;
+}
+
+static long tiles_of(int c, int width, int rows) {
+    int tw = 1, th = 1;
+    config_tile(c, &tw, &th);
+    return static_cast<long>((width + tw - 1) / tw) * ((rows + th - 1) / th);
+}
+
+int config_for(const lpaici_kernelset *ks, int width, int rows) {
+    int dev = 0, sms = 0, max_optin = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return default_config(ks);
+    std::vector<float> tuned;
+    {
+        std::lock_guard<std::mutex> lock(ks->mu);
+        const bool have = dev < static_cast<int>(ks->tuned_config.size()) && ks->tuned_config[dev] >= 0;
+        const bool timed = dev < static_cast<int>(ks->tuned_tile_ms.size()) && !ks->tuned_tile_ms[dev].empty();
+        if (have && !timed) return ks->tuned_config[dev];  // forced by lpaici_set_tile_config
+        if (timed) tuned = ks->tuned_tile_ms[dev];
+    }
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    int best = -1;
+    double best_ms = 0.0;
+    for (int c = 0; c < LPAICI_NUM_TILE_CONFIGS; c++) {
+        const int bps = cached_bps(ks, dev, c, max_optin);
+        const float tile_ms = tuned.empty() ? kTileMs[c] : tuned[c];
+        if (bps <= 0 || !(tile_ms > 0.0f)) continue;
+        const long slots = static_cast<long>(sms) * bps;
+        const double est = tile_ms * bps * static_cast<double>((tiles_of(c, width, rows) + slots - 1) / slots);
+        if (best < 0 || est < best_ms) {
+            best = c;
+            best_ms = est;
+        }
+    }
+    return best >= 0 ? best : default_config(ks);
 }
 
 static int check_params(float sigma_or_one, float gamma) {
@@ -37,7 +98,8 @@ static int check_params(float sigma_or_one, float gamma) {
 // Shared body of the forward entry points.
 static int forward_common(const lpaici_kernelset *ks, const float *d_in, int in_pitch, int width, int in_height,
                           int row_begin, int row_count, float *d_out, int out_pitch, const float *host_var,
-                          float sigma, float gamma, uint8_t *d_smap, cudaStream_t stream, int step = 1) {
+                          float sigma, float gamma, uint8_t *d_smap, cudaStream_t stream, int step = 1,
+                          int config = -1) {
     if (!ks || !d_in || !d_out) return set_error(LPAICI_ERR_INVALID_ARG, "forward: null kernel set or image pointer");
     if (width <= 0 || in_height <= 0 || row_count <= 0)
         return set_error(LPAICI_ERR_INVALID_ARG, "forward: non-positive size %d x %d", width, row_count);
@@ -70,7 +132,7 @@ static int forward_common(const lpaici_kernelset *ks, const float *d_in, int in_
     KernelTables tab;
     fill_tables(ks, host_var, sigma, gamma, &tab);
     tab.blob = blob;
-    return launch_forward(ks, img, tab, default_config(ks), stream);
+    return launch_forward(ks, img, tab, config >= 0 ? config : config_for(ks, width, row_count), stream);
 }
 
 // Every channel of an interleaved image (pixel (x, y), channel c at row y, float x * channels + c) as
@@ -218,8 +280,11 @@ int lpaici_denoise_host(const lpaici_kernelset *ks, const float *host_noisy, flo
     // Row bands, pipelined: the upload of the rows band b needs (its rows + R below) on s_in, its
     // forward on one of two compute streams (the next band's CTAs fill the SMs while this band's last
     // wave drains), its download on s_out.  With pinned host buffers the copies overlap the kernels.
+    // one configuration for all bands, chosen for the whole image: the bands' launches overlap on two
+    // streams, so the GPU sees one stream of tiles, not separate short launches
+    const int config = config_for(ks, width, height);
     int tile_h = 64;
-    lpaici_tile_config_desc(default_config(ks), nullptr, &tile_h, nullptr, nullptr);
+    lpaici_tile_config_desc(config, nullptr, &tile_h, nullptr, nullptr);
     const int R = ks->radius;
     int band = ((height + 7) / 8 + tile_h - 1) / tile_h * tile_h;
     if (band < tile_h) band = tile_h;
@@ -246,7 +311,7 @@ int lpaici_denoise_host(const lpaici_kernelset *ks, const float *host_noisy, flo
             break;
         }
         rc = forward_common(ks, b.in, width, width, height, r0, r1 - r0, b.out + static_cast<size_t>(r0) * width, width,
-                            nullptr, sigma, gamma, nullptr, sc);
+                            nullptr, sigma, gamma, nullptr, sc, 1, config);
         if (rc != LPAICI_OK) break;
         e = cudaEventRecord(b.ev_comp[i], sc);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(b.s_out, b.ev_comp[i], 0);
@@ -379,6 +444,7 @@ extern "C" int lpaici_autotune(lpaici_kernelset *ks, const float *d_sample, int 
     cudaEventCreate(&e1);
     float best_ms = 0.0f;
     int best = -1;
+    std::vector<float> config_ms(LPAICI_NUM_TILE_CONFIGS, -1.0f);
     for (int c = 0; rc == LPAICI_OK && c < LPAICI_NUM_TILE_CONFIGS; c++) {
         int crc = launch_forward(ks, img, tab, c, stream);  // warm-up
         if (crc != LPAICI_OK) {
@@ -399,6 +465,7 @@ extern "C" int lpaici_autotune(lpaici_kernelset *ks, const float *d_sample, int 
         cudaEventElapsedTime(&ms, e0, e1);
         ms /= reps;
         if (ms_out) ms_out[c] = ms;
+        config_ms[c] = ms;
         if (best < 0 || ms < best_ms) {
             best = c;
             best_ms = ms;
@@ -411,7 +478,24 @@ extern "C" int lpaici_autotune(lpaici_kernelset *ks, const float *d_sample, int 
     if (rc != LPAICI_OK) return rc;
     if (best < 0) return set_error(LPAICI_ERR_UNSUPPORTED, "no tile configuration fits this kernel set");
     if (best_config) *best_config = best;
-    return lpaici_set_tile_config(ks, best);
+    rc = lpaici_set_tile_config(ks, best);
+    if (rc != LPAICI_OK) return rc;
+    // per-tile times, for picking the configuration of other image sizes (config_for)
+    int dev = 0, sms = 0, max_optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    std::vector<float> tile_ms(LPAICI_NUM_TILE_CONFIGS, -1.0f);
+    for (int c = 0; c < LPAICI_NUM_TILE_CONFIGS; c++) {
+        const int bps = cached_bps(ks, dev, c, max_optin);
+        if (!(config_ms[c] > 0.0f) || bps <= 0) continue;
+        const long slots = static_cast<long>(sms) * bps;
+        tile_ms[c] = config_ms[c] / (bps * static_cast<float>((tiles_of(c, width, height) + slots - 1) / slots));
+    }
+    std::lock_guard<std::mutex> lock(ks->mu);
+    if (static_cast<int>(ks->tuned_tile_ms.size()) <= dev) ks->tuned_tile_ms.resize(dev + 1);
+    ks->tuned_tile_ms[dev] = tile_ms;
+    return LPAICI_OK;
 }
 
 extern "C" int lpaici_set_tile_config(lpaici_kernelset *ks, int config) {
@@ -426,5 +510,6 @@ extern "C" int lpaici_set_tile_config(lpaici_kernelset *ks, int config) {
         ks->tuned_config.resize(dev + 1, -1);
     }
     ks->tuned_config[dev] = config;
+    if (dev < static_cast<int>(ks->tuned_tile_ms.size())) ks->tuned_tile_ms[dev].clear();  // forced
     return LPAICI_OK;
 }

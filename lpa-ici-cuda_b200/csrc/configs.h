@@ -16,7 +16,12 @@
     X(6, 4, 2, 4)              \
     X(7, 5, 4, 4)              \
     X(8, 4, 5, 4)              \
-    X(9, 6, 4, 4)
+    X(9, 6, 4, 4)              \
+    X(10, 4, 6, 4)
 
-#define LPAICI_NUM_TILE_CONFIGS 10
+#define LPAICI_NUM_TILE_CONFIGS 11
 #define LPAICI_DEFAULT_TILE_CONFIG 0
+
+// Without autotuning, the first of these whose shared memory fits is used: the configurations in
+// order of their B200 time on the 4096^2 benchmark image (16x7 symmetric kernels), fastest first.
+#define LPAICI_TILE_PREFERENCE {10, 9, 8, 7, 0, 1, 2, 6, 3, 4, 5}

@@ -61,6 +61,44 @@ int launch_cfg(const ImageArgs &img, const KernelTables &tab, cudaStream_t strea
 #define LPAICI_FWD_CASE(idx, WX, WY, Q) \
     case idx: return launch_cfg<WX, WY, Q>(img, tab, stream);
 
+template <int WX, int WY, int Q>
+int blocks_per_sm(size_t smem) {
+    auto kern = lpaici_forward_kernel<WX, WY, Q>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, TileShape<WX, WY, Q>::kThreads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+int config_blocks_per_sm(int config, size_t smem) {
+#define LPAICI_BPS_CASE(idx, WX, WY, Q) \
+    case idx: return blocks_per_sm<WX, WY, Q>(smem);
+    switch (config) {
+        LPAICI_TILE_CONFIGS(LPAICI_BPS_CASE)
+        default: return 0;
+    }
+#undef LPAICI_BPS_CASE
+}
+
+void config_tile(int config, int *tile_w, int *tile_h) {
+#define LPAICI_TILE_CASE(idx, WX, WY, Q) \
+    case idx:                            \
+        *tile_w = 4 * (Q) * (WX);        \
+        *tile_h = 16 * (WY);             \
+        return;
+    switch (config) {
+        LPAICI_TILE_CONFIGS(LPAICI_TILE_CASE)
+        default: *tile_w = *tile_h = 1;
+    }
+#undef LPAICI_TILE_CASE
+}
+
 // Shared memory a tile configuration needs for a kernel set: blob + tables + the T8 tile.
 size_t config_smem(int config, int blob_words, int nk, int R) {
 #define LPAICI_SMEM_CASE(idx, WX, WY, Q)                                                   \

@@ -87,6 +87,10 @@ struct lpaici_kernelset {
     mutable std::vector<int *> dev_blob;
     mutable std::vector<int *> dev_adj_blob;
     mutable std::vector<int> tuned_config;  // per device, -1 = not tuned
+    // per device: ms one SM spends on one tile of each configuration, from lpaici_autotune (empty: not
+    // tuned, or a configuration forced by lpaici_set_tile_config); and CTAs per SM of each (0: unknown)
+    mutable std::vector<std::vector<float>> tuned_tile_ms;
+    mutable std::vector<std::vector<int>> blocks_per_sm;
 };
 
 namespace lpaici {
@@ -106,6 +110,13 @@ int launch_forward(const lpaici_kernelset *ks, const ImageArgs &img, const Kerne
 size_t config_smem(int config, int blob_words, int nk, int R);
 // The autotuned configuration of ks on the current device, else the first one that fits.
 int default_config(const lpaici_kernelset *ks);
+// The configuration expected to be fastest for one launch over width x rows pixels: per-tile time
+// (tuned, else a B200 table) times the waves of CTAs the image needs.  A forced configuration wins.
+int config_for(const lpaici_kernelset *ks, int width, int rows);
+// CTAs of the forward kernel of `config` that fit on one SM with `smem` bytes of shared memory.
+int config_blocks_per_sm(int config, size_t smem);
+// Tile width and height of a configuration.
+void config_tile(int config, int *tile_w, int *tile_h);
 // One image of a batch plan (batched.cu): out may be null (no estimate), smap and rden optional.
 struct BatchSpec {
     const float *noisy;

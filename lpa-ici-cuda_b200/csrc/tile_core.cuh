@@ -219,6 +219,9 @@ __device__ __forceinline__ void direction_sweep(int d, int S, unsigned valid, co
 #pragma unroll
         for (int m = 0; m < Q; m++) acc[m] = make_float2(0.0f, 0.0f);
         const int rb = s_blob[k], re = s_blob[k + 1];
+        // two runs per iteration for Q = 4: the compiler then keeps the 768-thread tiles within 80
+        // registers without spilling (measured: 24 warps per SM beat 20)
+#pragma unroll(Q == 4 ? 2 : 1)
         for (int r = rb; r < re; r++) {
             const int4 run = s_runs[r];
             conv_run<Q>(acc, lane_tile + run.x * pitch2 + run.y, s_wq + (run.w >> 1), run.z, nz);
