@@ -27,16 +27,19 @@ namespace lpaici {
 
 namespace {
 
-constexpr int kGatherP = 9;  // outputs per thread (odd: conflict-free scalar shared loads)
+constexpr int kGatherP = 9;  // output columns per thread (odd: conflict-free scalar shared loads)
 constexpr int kGatherWX = 2;
 constexpr int kGatherTW = kGatherWX * 4 * kGatherP;  // 72 output columns; 8 * WY rows (WY = 8: 64)
-// Two groups of 16 warps cover the same outputs, each with every other run of a kernel; their partial
-// sums are added at the end (1024 threads: twice the warps to hide shared-memory latency).
-constexpr int kGatherGroups = 2;
+// A warp covers 16 output rows x 36 columns: lane l owns rows y and y + 8 (y = l / 4 within the warp's
+// 8-row band) at 9 columns, and computes the two rows in the halves of packed f32x2 FMAs.  Four groups
+// of warps cover the same outputs, each with every fourth run of a kernel; their partial sums are added
+// at the end.
+constexpr int kGatherGroups = 4;
 template <int WY>
 struct GatherShape {
+    static_assert(WY % 2 == 0, "a warp covers 16 rows");
     static constexpr int kTH = 8 * WY;
-    static constexpr int kGroupThreads = 32 * kGatherWX * WY;
+    static constexpr int kGroupThreads = 32 * kGatherWX * (WY / 2);
     static constexpr int kThreads = kGatherGroups * kGroupThreads;
 };
 // Tile heights the host can choose (the tallest whose fields and mirrored kernels fit in shared memory).
@@ -75,31 +78,46 @@ __host__ __device__ inline int field_pitch(int need) {
     return p;
 }
 
-// acc[i] += sum_{j < len} w[j] * src[i + j] for the thread's P outputs (sliding window, FFMA).  Reads
-// src[0, len + P - 1).
+// d = a * b + c in each half, rounded on its own (the two halves of fmaf).
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
+        "fma.rn.f32x2 rd, ra, rb, rc;\n\t"
+        "mov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return d;
+}
+
+// acc[i] += sum_{j < len} w[j] * {src[i + j], src[i + j + pair]} for the thread's P output columns in
+// its two rows (sliding window).  Reads src[0, len + P - 1) and the same span at src + pair.
 template <int P>
-__device__ __forceinline__ void gather_run(float (&acc)[P], const float *__restrict__ src, const float *__restrict__ w,
-                                           int len) {
-    float win[P];
+__device__ __forceinline__ void gather_run(float2 (&acc)[P], const float *__restrict__ src, int pair,
+                                           const float *__restrict__ w, int len) {
+    const float *__restrict__ src2 = src + pair;
+    float2 win[P];
 #pragma unroll
-    for (int i = 0; i < P - 1; i++) win[i] = src[i];
+    for (int i = 0; i < P - 1; i++) win[i] = make_float2(src[i], src2[i]);
     int k = 0;
     for (; k + P <= len; k += P) {
 #pragma unroll
         for (int j = 0; j < P; j++) {
-            win[(j + P - 1) % P] = src[k + j + P - 1];
+            win[(j + P - 1) % P] = make_float2(src[k + j + P - 1], src2[k + j + P - 1]);
             const float wt = w[k + j];
+            const float2 w2 = make_float2(wt, wt);
 #pragma unroll
-            for (int i = 0; i < P; i++) acc[i] = fmaf(wt, win[(j + i) % P], acc[i]);
+            for (int i = 0; i < P; i++) acc[i] = fma2(w2, win[(j + i) % P], acc[i]);
         }
     }
 #pragma unroll
     for (int j = 0; j < P - 1; j++) {
         if (k + j >= len) break;
-        win[(j + P - 1) % P] = src[k + j + P - 1];
+        win[(j + P - 1) % P] = make_float2(src[k + j + P - 1], src2[k + j + P - 1]);
         const float wt = w[k + j];
+        const float2 w2 = make_float2(wt, wt);
 #pragma unroll
-        for (int i = 0; i < P; i++) acc[i] = fmaf(wt, win[(j + i) % P], acc[i]);
+        for (int i = 0; i < P; i++) acc[i] = fma2(w2, win[(j + i) % P], acc[i]);
     }
 }
 
@@ -131,7 +149,7 @@ __global__ void __launch_bounds__(GatherShape<WY>::kThreads, 1)
     const int gx0 = x0 - a.R, gy0 = y0 - a.R;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = kGatherThreads >> 5;
     const int group = threadIdx.x / kGroupThreads, gtid = threadIdx.x % kGroupThreads, gwarp = gtid >> 5;
-    const int ty = (gwarp / kGatherWX) * 8 + (lane >> 2);
+    const int ty = (gwarp / kGatherWX) * 16 + (lane >> 2);  // and ty + 8
     const int tx = (gwarp % kGatherWX) * 4 * P + (lane & 3) * P;
     const int4 *s_runs = reinterpret_cast<const int4 *>(s_blob + a.run_word);
     float *s_w = reinterpret_cast<float *>(s_blob + a.weight_word);
@@ -161,9 +179,10 @@ __global__ void __launch_bounds__(GatherShape<WY>::kThreads, 1)
         }
     }
 
-    float acc[P];
+    float2 acc[P];
 #pragma unroll
-    for (int i = 0; i < P; i++) acc[i] = 0.0f;
+    for (int i = 0; i < P; i++) acc[i] = make_float2(0.0f, 0.0f);
+    const int pair = 8 * a.pitch;
 
     for (int d = 0; d < a.D; d++) {
         __syncthreads();  // weights scaled; the previous direction's gathers are done with s_s / s_f
@@ -207,23 +226,39 @@ __global__ void __launch_bounds__(GatherShape<WY>::kThreads, 1)
             __syncthreads();
             for (int r = s_blob[k] + group; r < s_blob[k + 1]; r += kGatherGroups) {
                 const int4 run = s_runs[r];
-                gather_run<P>(acc, lane_f + run.x * a.pitch + run.y, s_w + run.w, run.z);
+                gather_run<P>(acc, lane_f + run.x * a.pitch + run.y, pair, s_w + run.w, run.z);
             }
             __syncthreads();  // before the next kernel's field overwrites s_f
         }
     }
-    // group 1 hands its partial sums to group 0 through s_f (free after the last barrier)
-    if (group == 1) {
+    // groups 1, 2, ... hand their partial sums to group 0 in turn through s_f (free after the last
+    // barrier); group 0 adds them in group order
+    float2 *s_h = reinterpret_cast<float2 *>(s_f);
+    for (int g = 1; g < kGatherGroups; g++) {
+        if (group == g) {
 #pragma unroll
-        for (int i = 0; i < P; i++) s_f[i * kGroupThreads + gtid] = acc[i];
+            for (int i = 0; i < P; i++) s_h[i * kGroupThreads + gtid] = acc[i];
+        }
+        __syncthreads();
+        if (group == 0) {
+#pragma unroll
+            for (int i = 0; i < P; i++) {
+                const float2 other = s_h[i * kGroupThreads + gtid];
+                acc[i] = make_float2(acc[i].x + other.x, acc[i].y + other.y);
+            }
+        }
+        __syncthreads();
     }
-    __syncthreads();
-    const int oy = y0 + ty;
-    if (group == 0 && oy < im.H) {
-        float *o = im.grad + static_cast<size_t>(oy) * im.grad_pitch + x0 + tx;
+    if (group == 0) {
 #pragma unroll
-        for (int i = 0; i < P; i++)
-            if (x0 + tx + i < im.W) o[i] = acc[i] + s_f[i * kGroupThreads + gtid];
+        for (int h = 0; h < 2; h++) {
+            const int oy = y0 + ty + 8 * h;
+            if (oy >= im.H) break;
+            float *o = im.grad + static_cast<size_t>(oy) * im.grad_pitch + x0 + tx;
+#pragma unroll
+            for (int i = 0; i < P; i++)
+                if (x0 + tx + i < im.W) o[i] = h == 0 ? acc[i].x : acc[i].y;
+        }
     }
 }
 
