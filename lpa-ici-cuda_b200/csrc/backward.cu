@@ -170,13 +170,14 @@ __global__ void __launch_bounds__(GatherShape<WY>::kThreads, 1)
         }
     }
     __syncthreads();
-    // alpha's 1/v_k moves into kernel k's weights: sum_t (w_t / v_k) u(p_t)
-    for (int k = threadIdx.x; k < nk; k += kGatherThreads) {
+    // alpha's 1/v_k moves into kernel k's weights: sum_t (w_t / v_k) u(p_t); a kernel's weights are
+    // contiguous, one warp scales them
+    for (int k = warp; k < nk; k += nwarps) {
+        const int r0 = s_blob[k], r1 = s_blob[k + 1];
+        if (r0 == r1) continue;
+        const int w0 = s_runs[r0].w, w1 = s_runs[r1 - 1].w + s_runs[r1 - 1].z;
         const float rv = rvar_k[k];
-        for (int r = s_blob[k]; r < s_blob[k + 1]; r++) {
-            const int4 run = s_runs[r];
-            for (int j = 0; j < run.z; j++) s_w[run.w + j] *= rv;
-        }
+        for (int i = w0 + lane; i < w1; i += 32) s_w[i] *= rv;
     }
 
     float2 acc[P];
@@ -224,9 +225,15 @@ __global__ void __launch_bounds__(GatherShape<WY>::kThreads, 1)
                 }
             }
             __syncthreads();
-            for (int r = s_blob[k] + group; r < s_blob[k + 1]; r += kGatherGroups) {
+            // the run descriptors are the same in every lane: reduced, they are known warp-uniform, so
+            // the loop and the tail's exits branch without reconvergence bookkeeping
+            const int r_end = __reduce_max_sync(0xffffffffu, s_blob[k + 1]);
+            for (int r = __reduce_max_sync(0xffffffffu, s_blob[k] + group); r < r_end; r += kGatherGroups) {
                 const int4 run = s_runs[r];
-                gather_run<P>(acc, lane_f + run.x * a.pitch + run.y, pair, s_w + run.w, run.z);
+                const int off = __reduce_max_sync(0xffffffffu, run.x * a.pitch + run.y);
+                const int wo = __reduce_max_sync(0xffffffffu, run.w);
+                const int len = __reduce_max_sync(0xffffffffu, run.z);
+                gather_run<P>(acc, lane_f + off, pair, s_w + wo, len);
             }
             __syncthreads();  // before the next kernel's field overwrites s_f
         }
