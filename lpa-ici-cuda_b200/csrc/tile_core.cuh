@@ -89,9 +89,9 @@ __host__ __device__ inline int table_words(int nk) { return (3 * nk + 3) & ~3; }
 // the Q pixel pairs m accumulate w * column (k + J + m).  Weights come two taps per float4.
 #define LPAICI_STEP(J)                                                                               \
     {                                                                                                \
-        if (((J) & 1) == 0) wv = wq[(k + (J)) >> 1];                                                 \
+        if (((J) & 1) == 0) wv = wq[(J) >> 1];                                                       \
         const float2 w2 = ((J) & 1) ? make_float2(wv.z, wv.w) : make_float2(wv.x, wv.y);             \
-        win[((J) + Q - 1) % Q] = src[k + (J) + Q - 1];                                               \
+        win[((J) + Q - 1) % Q] = src[(J) + Q - 1];                                                   \
         _Pragma("unroll") for (int m = 0; m < Q; m++) acc[m] = add2(acc[m], prod2(w2, win[((J) + m) % Q], nz)); \
     }
 
@@ -101,7 +101,7 @@ __host__ __device__ inline int table_words(int nk) { return (3 * nk + 3) & ~3; }
 // The last len % Q taps: their window columns and weights are loaded before any of them is used --
 // unconditionally, which stays inside the tile (pitch2 carries Q spare columns) and the blob (the
 // weights carry spare taps) -- and only the arithmetic of each tap is guarded, so the tail pays no
-// load latency per tap.
+// load latency per tap.  src and wq advance with the taps, so every load has a constant offset.
 template <int Q>
 __device__ __forceinline__ void conv_run(float2 (&acc)[Q], const float2 *__restrict__ src,
                                          const float4 *__restrict__ wq, int len, float2 nz) {
@@ -109,19 +109,19 @@ __device__ __forceinline__ void conv_run(float2 (&acc)[Q], const float2 *__restr
     float4 wv;
 #pragma unroll
     for (int i = 0; i < Q - 1; i++) win[i] = src[i];
-    int k = 0;
-    for (; k + Q <= len; k += Q) {
+    int rem = len;
+    for (; rem >= Q; rem -= Q, src += Q, wq += Q / 2) {
 #pragma unroll
         for (int J = 0; J < Q; J++) LPAICI_STEP(J)
     }
-    const int rem = len - k;  // 0 .. Q-1, warp-uniform
+    // rem: 0 .. Q-1, warp-uniform
     if (rem > 0) {
         float2 tail[Q - 1];
         float4 tw[Q / 2];
 #pragma unroll
-        for (int J = 0; J < Q - 1; J++) tail[J] = src[k + J + Q - 1];
+        for (int J = 0; J < Q - 1; J++) tail[J] = src[J + Q - 1];
 #pragma unroll
-        for (int i = 0; i < Q / 2; i++) tw[i] = wq[(k >> 1) + i];
+        for (int i = 0; i < Q / 2; i++) tw[i] = wq[i];
 #pragma unroll
         for (int J = 0; J < Q - 1; J++) {
             if (J < rem) {
