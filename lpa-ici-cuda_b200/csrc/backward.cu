@@ -91,7 +91,8 @@ __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
 }
 
 // acc[i] += sum_{j < len} w[j] * {src[i + j], src[i + j + pair]} for the thread's P output columns in
-// its two rows (sliding window).  Reads src[0, len + P - 1) and the same span at src + pair.
+// its two rows (sliding window).  Reads src[0, len + P - 1) and the same span at src + pair.  The
+// pointers advance with the taps, so every load has a constant offset.
 template <int P>
 __device__ __forceinline__ void gather_run(float2 (&acc)[P], const float *__restrict__ src, int pair,
                                            const float *__restrict__ w, int len) {
@@ -99,12 +100,11 @@ __device__ __forceinline__ void gather_run(float2 (&acc)[P], const float *__rest
     float2 win[P];
 #pragma unroll
     for (int i = 0; i < P - 1; i++) win[i] = make_float2(src[i], src2[i]);
-    int k = 0;
-    for (; k + P <= len; k += P) {
+    for (; len >= P; len -= P, src += P, src2 += P, w += P) {
 #pragma unroll
         for (int j = 0; j < P; j++) {
-            win[(j + P - 1) % P] = make_float2(src[k + j + P - 1], src2[k + j + P - 1]);
-            const float wt = w[k + j];
+            win[(j + P - 1) % P] = make_float2(src[j + P - 1], src2[j + P - 1]);
+            const float wt = w[j];
             const float2 w2 = make_float2(wt, wt);
 #pragma unroll
             for (int i = 0; i < P; i++) acc[i] = fma2(w2, win[(j + i) % P], acc[i]);
@@ -112,9 +112,9 @@ __device__ __forceinline__ void gather_run(float2 (&acc)[P], const float *__rest
     }
 #pragma unroll
     for (int j = 0; j < P - 1; j++) {
-        if (k + j >= len) break;
-        win[(j + P - 1) % P] = make_float2(src[k + j + P - 1], src2[k + j + P - 1]);
-        const float wt = w[k + j];
+        if (j >= len) break;
+        win[(j + P - 1) % P] = make_float2(src[j + P - 1], src2[j + P - 1]);
+        const float wt = w[j];
         const float2 w2 = make_float2(wt, wt);
 #pragma unroll
         for (int i = 0; i < P; i++) acc[i] = fma2(w2, win[(j + i) % P], acc[i]);
