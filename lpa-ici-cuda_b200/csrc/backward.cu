@@ -78,6 +78,21 @@ __host__ __device__ inline int field_pitch(int need) {
     return p;
 }
 
+// Copies the mirrored blob like stage_words and folds each run's (dy, dx0) into its offset
+// dy * pitch + dx0 in the field, on the way: the run becomes (offset, 0, len, weight index).  Runs
+// occupy words [run_word, weight_word).
+__device__ __forceinline__ void stage_adj_blob(int *dst, const int *__restrict__ src, int words, int run_word,
+                                               int weight_word, int pitch) {
+    const int4 *s = reinterpret_cast<const int4 *>(src);
+    int4 *d = reinterpret_cast<int4 *>(dst);
+    const int r0 = run_word >> 2, r1 = weight_word >> 2;
+    for (int i = threadIdx.x; i < (words >> 2); i += blockDim.x) {
+        int4 v = __ldg(s + i);
+        if (i >= r0 && i < r1) v = make_int4(v.x * pitch + v.y, 0, v.z, v.w);
+        d[i] = v;
+    }
+}
+
 // d = a * b + c in each half, rounded on its own (the two halves of fmaf).
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
     float2 d;
@@ -157,7 +172,7 @@ __global__ void __launch_bounds__(GatherShape<WY>::kThreads, 1)
     const int groups = a.pitch >> 2;
     const int nk = a.D * a.S;
 
-    stage_words(s_blob, a.blob, a.blob_words);
+    stage_adj_blob(s_blob, a.blob, a.blob_words, a.run_word, a.weight_word, a.pitch);
     for (int r = warp; r < a.rows; r += nwarps) {  // one warp per row, lanes along it
         const int gy = gy0 + r;
         const bool row_ok = gy >= 0 && gy < im.H;
@@ -230,7 +245,7 @@ __global__ void __launch_bounds__(GatherShape<WY>::kThreads, 1)
             const int r_end = __reduce_max_sync(0xffffffffu, s_blob[k + 1]);
             for (int r = __reduce_max_sync(0xffffffffu, s_blob[k] + group); r < r_end; r += kGatherGroups) {
                 const int4 run = s_runs[r];
-                const int off = __reduce_max_sync(0xffffffffu, run.x * a.pitch + run.y);
+                const int off = __reduce_max_sync(0xffffffffu, run.x);  // dy * pitch + dx0: stage_adj_blob
                 const int wo = __reduce_max_sync(0xffffffffu, run.w);
                 const int len = __reduce_max_sync(0xffffffffu, run.z);
                 gather_run<P>(acc, lane_f + off, pair, s_w + wo, len);

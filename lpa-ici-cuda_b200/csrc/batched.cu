@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(32 * WX * WY, 1)
     float2 *s_tile = reinterpret_cast<float2 *>(smem + a.blob_words + table_words(nk));
     const TileGeom g = TileGeom::make(Shape::kTileW, Shape::kTileH, a.R, Q);
 
-    stage_words(s_blob, a.blob, a.blob_words);
+    stage_blob(s_blob, a.blob, a.blob_words, a.run_word, a.weight_word, g.pitch2);
     int cur_image = -1;
     for (;;) {
         if (threadIdx.x == 0) s_item = static_cast<int>(atomicAdd(a.counter, 1u));

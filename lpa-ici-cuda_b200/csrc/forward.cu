@@ -23,7 +23,7 @@ __global__ void __launch_bounds__(32 * WX * WY, 1)
     const TileGeom g = TileGeom::make(Shape::kTileW, Shape::kTileH, tab.R, Q);
     const int x0 = blockIdx.x * Shape::kTileW, y0 = blockIdx.y * Shape::kTileH;
 
-    stage_words(s_blob, tab.blob, tab.blob_words);
+    stage_blob(s_blob, tab.blob, tab.blob_words, tab.run_word, tab.weight_word, g.pitch2);
     stage_tables(s_tab, tab.var, tab.thr, nk);
     load_tile(s_tile, img, x0, y0, g);
     __syncthreads();

@@ -143,6 +143,21 @@ __device__ __forceinline__ void stage_words(int *dst, const int *__restrict__ sr
     for (int i = threadIdx.x; i < (words >> 2); i += blockDim.x) d[i] = __ldg(s + i);
 }
 
+// Copies the forward blob like stage_words and rewrites each run (row, col, len, w) on the way into
+// (row * pitch2 + col, len, w / 2, 0): its first input pair as an offset into the tile and its first
+// duplicated weight pair as a float4 index.  Runs occupy words [run_word, weight_word).
+__device__ __forceinline__ void stage_blob(int *dst, const int *__restrict__ src, int words, int run_word,
+                                           int weight_word, int pitch2) {
+    const int4 *s = reinterpret_cast<const int4 *>(src);
+    int4 *d = reinterpret_cast<int4 *>(dst);
+    const int r0 = run_word >> 2, r1 = weight_word >> 2;
+    for (int i = threadIdx.x; i < (words >> 2); i += blockDim.x) {
+        int4 v = __ldg(s + i);
+        if (i >= r0 && i < r1) v = make_int4(v.x * pitch2 + v.y, v.z, v.w >> 1, 0);
+        d[i] = v;
+    }
+}
+
 // var, thr and rvar = 1/var (correctly rounded, the reference's 1.0f / var_d) into shared memory.
 __device__ __forceinline__ void stage_tables(float *s_tab, const float *var, const float *thr, int nk) {
     for (int i = threadIdx.x; i < nk; i += blockDim.x) {
@@ -199,7 +214,7 @@ using ScaleBits = typename std::conditional<(8 * Q <= 32), unsigned, unsigned lo
 // the index is the count of accepted scales after it.  Warp-uniform scale loop; it ends when every
 // valid pixel of the warp has stopped.
 template <int Q>
-__device__ __forceinline__ void direction_sweep(int d, int S, unsigned valid, const float2 *lane_tile, int pitch2,
+__device__ __forceinline__ void direction_sweep(int d, int S, unsigned valid, const float2 *lane_tile,
                                                 const int *s_blob, const int4 *s_runs, const float4 *s_wq,
                                                 const float *s_thr, float2 nz, float2 (&best)[Q], ScaleBits<Q> &sidx) {
     float lo[2 * Q], hi[2 * Q];
@@ -223,8 +238,8 @@ __device__ __forceinline__ void direction_sweep(int d, int S, unsigned valid, co
         // registers without spilling (measured: 24 warps per SM beat 20)
 #pragma unroll(Q == 4 ? 2 : 1)
         for (int r = rb; r < re; r++) {
-            const int4 run = s_runs[r];
-            conv_run<Q>(acc, lane_tile + run.x * pitch2 + run.y, s_wq + (run.w >> 1), run.z, nz);
+            const int4 run = s_runs[r];  // (tile offset, len, float4 weight index): see stage_blob
+            conv_run<Q>(acc, lane_tile + run.x, s_wq + run.z, run.y, nz);
         }
         const float thr = s_thr[k];
         const ScaleBits<Q> step = s > 0 ? 1 : 0;
@@ -275,7 +290,7 @@ __device__ __forceinline__ void sweep_tile(const ImageArgs &img, int x0, int y0,
     for (int d = 0; d < D; d++) {
         float2 best[Q];
         ScaleBits<Q> sidx;
-        direction_sweep<Q>(d, S, valid, lane_tile, g.pitch2, s_blob, s_runs, s_wq, s_thr, nz, best, sidx);
+        direction_sweep<Q>(d, S, valid, lane_tile, s_blob, s_runs, s_wq, s_thr, nz, best, sidx);
 #pragma unroll
         for (int m = 0; m < Q; m++) {
             const float2 r = make_float2(s_rvar[d * S + static_cast<int>((sidx >> (8 * m)) & 15)],
