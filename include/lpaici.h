@@ -155,7 +155,9 @@ typedef struct {
 
 typedef struct {
     int use_graph;   /* nonzero: capture the launch sequence in a CUDA graph at plan time, replay on run */
-    int tile_config; /* -1: the autotuned choice for this kernel set and device; else an index < lpaici_num_tile_configs() */
+    int tile_config; /* -1: the configuration expected fastest for these images (per-tile times, autotuned
+                      * or built in, times the waves of the whole tile queue); else an index
+                      * < lpaici_num_tile_configs() */
 } lpaici_batch_options;
 
 typedef struct lpaici_batch lpaici_batch;

@@ -657,7 +657,15 @@ extern "C" int lpaici_backward_batch_create(const lpaici_kernelset *ks, const lp
     b->ga.items = reinterpret_cast<const int2 *>(base + item_off);
     b->grid = static_cast<unsigned>(total_tiles);
 
-    const int config = (opts && opts->tile_config >= 0) ? opts->tile_config : default_config(ks);
+    int config = opts ? opts->tile_config : -1;
+    if (config < 0) {
+        std::vector<int> w(n), h(n);
+        for (int i = 0; i < n; i++) {
+            w[i] = specs[i].width;
+            h[i] = specs[i].height;
+        }
+        config = config_for_images(ks, w.data(), h.data(), n);
+    }
     rc = batch_plan_create(ks, specs.data(), n, config, false, stream, &b->select);
     if (rc != LPAICI_OK) {
         backward_batch_free(b);

@@ -309,7 +309,15 @@ int lpaici_batch_create(const lpaici_kernelset *ks, const lpaici_image *images, 
         specs[i] = BatchSpec{im.noisy, im.denoised, im.scale_map, nullptr, im.width, im.height, im.noisy_pitch,
                              im.out_pitch, im.sigma, im.gamma};
     }
-    const int config = (opts && opts->tile_config >= 0) ? opts->tile_config : default_config(ks);
+    int config = opts ? opts->tile_config : -1;
+    if (config < 0) {
+        std::vector<int> w(n), h(n);
+        for (int i = 0; i < n; i++) {
+            w[i] = specs[i].width;
+            h[i] = specs[i].height;
+        }
+        config = config_for_images(ks, w.data(), h.data(), n);
+    }
     return batch_plan_create(ks, specs.data(), n, config, opts && opts->use_graph,
                              reinterpret_cast<cudaStream_t>(stream_), out);
 }

@@ -58,7 +58,7 @@ static long tiles_of(int c, int width, int rows) {
     return static_cast<long>((width + tw - 1) / tw) * ((rows + th - 1) / th);
 }
 
-int config_for(const lpaici_kernelset *ks, int width, int rows) {
+int config_for_images(const lpaici_kernelset *ks, const int *widths, const int *rows, int n) {
     int dev = 0, sms = 0, max_optin = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return default_config(ks);
     std::vector<float> tuned;
@@ -77,8 +77,10 @@ int config_for(const lpaici_kernelset *ks, int width, int rows) {
         const int bps = cached_bps(ks, dev, c, max_optin);
         const float tile_ms = tuned.empty() ? kTileMs[c] : tuned[c];
         if (bps <= 0 || !(tile_ms > 0.0f)) continue;
+        long tiles = 0;
+        for (int i = 0; i < n; i++) tiles += tiles_of(c, widths[i], rows[i]);
         const long slots = static_cast<long>(sms) * bps;
-        const double est = tile_ms * bps * static_cast<double>((tiles_of(c, width, rows) + slots - 1) / slots);
+        const double est = tile_ms * bps * static_cast<double>((tiles + slots - 1) / slots);
         if (best < 0 || est < best_ms) {
             best = c;
             best_ms = est;
@@ -86,6 +88,8 @@ int config_for(const lpaici_kernelset *ks, int width, int rows) {
     }
     return best >= 0 ? best : default_config(ks);
 }
+
+int config_for(const lpaici_kernelset *ks, int width, int rows) { return config_for_images(ks, &width, &rows, 1); }
 
 static int check_params(float sigma_or_one, float gamma) {
     if (!(sigma_or_one > 0.0f) || !std::isfinite(sigma_or_one))

@@ -113,6 +113,8 @@ int default_config(const lpaici_kernelset *ks);
 // The configuration expected to be fastest for one launch over width x rows pixels: per-tile time
 // (tuned, else a B200 table) times the waves of CTAs the image needs.  A forced configuration wins.
 int config_for(const lpaici_kernelset *ks, int width, int rows);
+// The same for one launch over n images (a batched plan's tile queue): the images' tiles add up.
+int config_for_images(const lpaici_kernelset *ks, const int *widths, const int *rows, int n);
 // CTAs of the forward kernel of `config` that fit on one SM with `smem` bytes of shared memory.
 int config_blocks_per_sm(int config, size_t smem);
 // Tile width and height of a configuration.
