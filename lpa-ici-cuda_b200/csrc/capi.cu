@@ -290,10 +290,26 @@ int lpaici_denoise_host(const lpaici_kernelset *ks, const float *host_noisy, flo
     int tile_h = 64;
     lpaici_tile_config_desc(config, nullptr, &tile_h, nullptr, nullptr);
     const int R = ks->radius;
-    int band = ((height + 7) / 8 + tile_h - 1) / tile_h * tile_h;
-    if (band < tile_h) band = tile_h;
-    while ((height + band - 1) / band > kMaxBands) band += tile_h;
-    const int nb = (height + band - 1) / band;
+    // band i covers rows [edge[i], edge[i + 1]): the first is one tile row high and the last one or two,
+    // so the upload before the first forward and the download after the last one are short; the
+    // bands between are about an eighth of the image
+    int edge[kMaxBands + 1];
+    int nb = 0;
+    if (height <= 3 * tile_h) {
+        edge[0] = 0;
+        edge[1] = height;
+        nb = 1;
+    } else {
+        const int last = tile_h + (height - 2 * tile_h) % tile_h;  // the middle bands stay whole tile rows
+        const int mid = height - tile_h - last;
+        int band = ((height + 7) / 8 + tile_h - 1) / tile_h * tile_h;
+        while (2 + (mid + band - 1) / band > kMaxBands) band += tile_h;
+        edge[0] = 0;
+        edge[1] = tile_h;
+        nb = 1;
+        for (int r = tile_h; r < tile_h + mid; r += band) edge[++nb] = std::min(tile_h + mid, r + band);
+        edge[++nb] = height;
+    }
     HostBuffers &b = t_bufs;
     e = cudaEventRecord(b.ev_start, stream);
     for (cudaStream_t st : {b.s_in, b.s_out, b.s_comp[0], b.s_comp[1]})
@@ -301,7 +317,7 @@ int lpaici_denoise_host(const lpaici_kernelset *ks, const float *host_noisy, flo
     if (e != cudaSuccess) return cuda_error(e, "lpaici_denoise_host: stream order");
     int copied = 0;  // input rows [0, copied) uploaded
     for (int i = 0; i < nb && rc == LPAICI_OK; i++) {
-        const int r0 = i * band, r1 = std::min(height, r0 + band), need = std::min(height, r1 + R);
+        const int r0 = edge[i], r1 = edge[i + 1], need = std::min(height, r1 + R);
         if (need > copied) {
             e = cudaMemcpyAsync(b.in + static_cast<size_t>(copied) * width, host_noisy + static_cast<size_t>(copied) * width,
                                 sizeof(float) * width * static_cast<size_t>(need - copied), cudaMemcpyHostToDevice, b.s_in);
