@@ -208,10 +208,12 @@ def test_error_against_fp64():
     assert abs(lpaici.psnr(clean, out) - psnr64) <= 0.01
 
 
-@pytest.mark.parametrize("W,H", [(1000, 1500), (517, 81), (33, 1), (2048, 4097)])
+@pytest.mark.parametrize("W,H", [(1000, 1500), (517, 81), (33, 1), (2048, 4097), (300, 289), (640, 385)])
 def test_host_engine_bands_equal_device_path(W, H):
-    """lpaici_denoise_host pipelines row bands (upload, forward, download on separate streams); its
-    result equals the single device launch bit for bit, from pageable and from pinned host buffers."""
+    """lpaici_denoise_host pipelines row bands (upload, forward, download on separate streams; a
+    one-tile-row band first, one or two tile rows last, an eighth of the image between); its result
+    equals the single device launch bit for bit, from pageable and from pinned host buffers.  The
+    sizes give one band, three bands just past three tile rows, and many bands with a remainder."""
     import torch
 
     ks = lpaici.KernelSet.load(kernel_file(SYM))
