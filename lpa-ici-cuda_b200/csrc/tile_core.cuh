@@ -95,13 +95,55 @@ __host__ __device__ inline int table_words(int nk) { return (3 * nk + 3) & ~3; }
         _Pragma("unroll") for (int m = 0; m < Q; m++) acc[m] = add2(acc[m], prod2(w2, win[((J) + m) % Q], nz)); \
     }
 
+// The last N (< Q) taps of a run: their window columns and weights are loaded before any of them is
+// used, so the tail pays no load latency per tap.
+template <int Q, int N>
+__device__ __forceinline__ void conv_tail(float2 (&acc)[Q], float2 (&win)[Q], const float2 *__restrict__ src,
+                                          const float4 *__restrict__ wq, float2 nz) {
+    float2 tail[N];
+    float4 tw[(N + 1) / 2];
+#pragma unroll
+    for (int J = 0; J < N; J++) tail[J] = src[J + Q - 1];
+#pragma unroll
+    for (int i = 0; i < (N + 1) / 2; i++) tw[i] = wq[i];
+#pragma unroll
+    for (int J = 0; J < N; J++) {
+        const float2 w2 = (J & 1) ? make_float2(tw[J >> 1].z, tw[J >> 1].w) : make_float2(tw[J >> 1].x, tw[J >> 1].y);
+        win[(J + Q - 1) % Q] = tail[J];
+#pragma unroll
+        for (int m = 0; m < Q; m++) acc[m] = add2(acc[m], prod2(w2, win[(J + m) % Q], nz));
+    }
+}
+
+template <int Q>
+__device__ __forceinline__ void conv_tail_dispatch(int rem, float2 (&acc)[Q], float2 (&win)[Q],
+                                                   const float2 *__restrict__ src, const float4 *__restrict__ wq,
+                                                   float2 nz) {
+    if constexpr (Q == 4) {
+        switch (rem) {
+            case 1: conv_tail<Q, 1>(acc, win, src, wq, nz); break;
+            case 2: conv_tail<Q, 2>(acc, win, src, wq, nz); break;
+            default: conv_tail<Q, 3>(acc, win, src, wq, nz); break;
+        }
+    } else {
+        static_assert(Q == 8, "tile configurations use Q = 4 or 8");
+        switch (rem) {
+            case 1: conv_tail<Q, 1>(acc, win, src, wq, nz); break;
+            case 2: conv_tail<Q, 2>(acc, win, src, wq, nz); break;
+            case 3: conv_tail<Q, 3>(acc, win, src, wq, nz); break;
+            case 4: conv_tail<Q, 4>(acc, win, src, wq, nz); break;
+            case 5: conv_tail<Q, 5>(acc, win, src, wq, nz); break;
+            case 6: conv_tail<Q, 6>(acc, win, src, wq, nz); break;
+            default: conv_tail<Q, 7>(acc, win, src, wq, nz); break;
+        }
+    }
+}
+
 // acc[m] += sum_{j < len} {w_j, w_j} * src[m + j], tap by tap in order, for the Q pixel pairs.
 // src: the run's first column in T8 (row already chosen); wq: the run's duplicated weights as
 // float4 {w_2i, w_2i, w_2i+1, w_2i+1}.
-// The last len % Q taps: their window columns and weights are loaded before any of them is used --
-// unconditionally, which stays inside the tile (pitch2 carries Q spare columns) and the blob (the
-// weights carry spare taps) -- and only the arithmetic of each tap is guarded, so the tail pays no
-// load latency per tap.  src and wq advance with the taps, so every load has a constant offset.
+// The last len % Q taps go to a tail of exactly that many taps (conv_tail): one warp-uniform
+// dispatch, no test per tap.  src and wq advance with the taps, so every load has a constant offset.
 template <int Q>
 __device__ __forceinline__ void conv_run(float2 (&acc)[Q], const float2 *__restrict__ src,
                                          const float4 *__restrict__ wq, int len, float2 nz) {
@@ -114,25 +156,8 @@ __device__ __forceinline__ void conv_run(float2 (&acc)[Q], const float2 *__restr
 #pragma unroll
         for (int J = 0; J < Q; J++) LPAICI_STEP(J)
     }
-    // rem: 0 .. Q-1, warp-uniform
-    if (rem > 0) {
-        float2 tail[Q - 1];
-        float4 tw[Q / 2];
-#pragma unroll
-        for (int J = 0; J < Q - 1; J++) tail[J] = src[J + Q - 1];
-#pragma unroll
-        for (int i = 0; i < Q / 2; i++) tw[i] = wq[i];
-#pragma unroll
-        for (int J = 0; J < Q - 1; J++) {
-            if (J < rem) {
-                const float2 w2 = (J & 1) ? make_float2(tw[J >> 1].z, tw[J >> 1].w)
-                                          : make_float2(tw[J >> 1].x, tw[J >> 1].y);
-                win[(J + Q - 1) % Q] = tail[J];
-#pragma unroll
-                for (int m = 0; m < Q; m++) acc[m] = add2(acc[m], prod2(w2, win[(J + m) % Q], nz));
-            }
-        }
-    }
+    // rem: 0 .. Q-1, warp-uniform: one dispatch to a tail of exactly rem taps
+    if (rem > 0) conv_tail_dispatch<Q>(rem, acc, win, src, wq, nz);
 }
 #undef LPAICI_STEP
 
