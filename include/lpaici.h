@@ -144,7 +144,7 @@ int lpaici_forward_channels(const lpaici_kernelset *ks, const float *d_noisy, in
                             int out_pitch, int width, int height, int channels, float sigma, float gamma,
                             lpaici_stream_t stream);
 
-/* ---- batched forward: images of uneven sizes, sigmas and gammas in one persistent launch ----- */
+/* ---- batched forward: images of uneven sizes, sigmas and gammas in one launch ---------------- */
 typedef struct {
     const float *noisy;  /* device, width x height, pitch noisy_pitch floats */
     float *denoised;     /* device, width x height, pitch out_pitch floats */
@@ -231,7 +231,7 @@ typedef struct {
 
 typedef struct lpaici_backward_batch lpaici_backward_batch;
 
-/* Plans the adjoint of many images: pass A (selection) as one persistent launch over all images'
+/* Plans the adjoint of many images: pass A (selection) as one launch over all images'
  * tiles (the forward batch kernel writing s* and 1/den into memory the plan owns, D+4 bytes per
  * pixel), pass B (gather) as one launch over all images' tiles; with use_graph both are captured in
  * one CUDA graph.  Gradients equal lpaici_backward's, image by image, bit for bit.  The pointers are

@@ -1,4 +1,4 @@
-"""Batched persistent forward: images of uneven sizes, sigmas and gammas in one launch must give, image
+"""Batched forward: images of uneven sizes, sigmas and gammas in one launch must give, image
 by image, exactly the single-image result (which is bit-exact with the reference)."""
 import numpy as np
 import pytest
@@ -36,7 +36,7 @@ def test_batch_equals_single(setup, use_graph):
     torch, ks, ko, imgs, sig, gam, singles = setup
     outs = [torch.full_like(x, float("nan")) for x in imgs]
     b = lpaici.Batch(ks, imgs, outs, sig, gam, use_graph=use_graph)
-    for rep in range(3):  # reruns reuse the plan (the queue counter is reset every run)
+    for rep in range(3):  # reruns reuse the plan
         for o in outs:
             o.fill_(float("nan"))
         b.run()
