@@ -21,7 +21,7 @@ rank's time.
             one 256x256 crop of the benchmark image per thread; its naive engine (v0_0) beside it
   parity    the GPU image against those reference outputs, bit for bit, on every crop pixel whose
             neighbourhood lies inside its crop
-  extra     batched persistent forward over 64 images (sides U[256,2048], sigma U[10,40]/255, gamma
+  extra     batched forward (one launch) over 64 images (sides U[256,2048], sigma U[10,40]/255, gamma
             U[1.5,2.5]) in a CUDA graph, and the adjoint on 8 x 1024^2, each against the plain forward
             on the same images; forward and adjoint on one 8192^2 image with the gaussian m=(2,0)
             kernels (sigma 25/255, gamma 1.5); adjoint checked by sum(g*out) = sum(grad*x)
@@ -375,7 +375,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         peak = fp32_peak()
     if rank == 0 and world == 1 and not args.no_extras:
         extra = run_extras(torch, lpaici, ks, args, flush)
-        # the persistent batched plan on the benchmark image itself, beside the plain launch
+        # the batched plan on the benchmark image itself, beside the plain launch
         outb = torch.empty_like(x)
         plan = lpaici.Batch(ks, [x], [outb], [SIGMA], [GAMMA], use_graph=True)
         b_ms = time_launches(torch, plan.run, args.steps, 1, flush)
@@ -527,7 +527,7 @@ def run_extras(torch, lpaici, ks, args, flush) -> dict:
                     "value": m * 1024 * 1024 / (np.mean(ab_ms) * 1e-3) / 1e6,
                     "forward_same_images": m * 1024 * 1024 / (np.mean(fb_ms) * 1e-3) / 1e6,
                     "adjoint_over_forward_time": float(np.mean(ab_ms) / np.mean(fb_ms)),
-                    "how": "batched plans (one selection + one gather launch; one persistent forward launch), "
+                    "how": "batched plans (one selection + one gather launch; one forward launch), "
                            "CUDA graphs",
                     "bit_equal_to_single": bool(batched_same),
                     "single_image_calls": {"value": m * 1024 * 1024 / (np.mean(a_ms) * 1e-3) / 1e6,
