@@ -91,8 +91,8 @@ static int finish_kernelset(lpaici_kernelset *ks) {
         n2 += (ks->run_len[r] + 1) & ~1;
     }
     L.n_wdup = n2;
-    // 16 spare {0, 0} taps after the last run: the speculative tail loads of the kernels read up to
-    // 8 taps past a run's end
+    // 16 spare {0, 0} taps after the last run, a margin: the kernels' weight loads stay within each
+    // run's taps and its even-length padding
     L.total_words = (L.weight_word + 2 * (n2 + 16) + 3) & ~3;
     ks->blob.assign(L.total_words, 0);
     for (int k = 0; k < nk; k++) ks->blob[k] = ks->k_first_run[k];

@@ -69,7 +69,8 @@ struct TileShape {
 };
 
 // Shared-memory geometry of a tile for radius R and Q column pairs per thread: tile_w + 2R columns
-// of halo'd input plus Q spare columns read (never used) by conv_run's speculative tail loads.
+// of halo'd input plus Q spare columns, a margin no load reaches (the last column a run's window
+// reads is tile_w + 2R - 1).
 struct TileGeom {
     int R, pitch2, pairs;  // pairs: number of T8 rows
     __host__ __device__ static TileGeom make(int tile_w, int tile_h, int R, int Q) {
