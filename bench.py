@@ -57,9 +57,12 @@ SIGMA = float(np.float32(20.0) / np.float32(255.0))
 GAMMA = 2.0
 SEED = 20250910
 SIZE = 4096
-# DRAM bytes of one forward launch on the 4096^2 workload, read + written, from an ncu capture
-# (dram__bytes_read.sum + dram__bytes_write.sum): the halo re-reads are served by L2.
+# DRAM bytes of one forward launch on the 4096^2 workload, read + written, from the ncu capture in
+# profiles/forward_4096_sym.md (dram__bytes_read.sum + dram__bytes_write.sum; the halo re-reads are
+# served by L2), valid for the tile configurations listed (the two 768-thread shapes, which stage the
+# same halo'd tiles): reported only when the run uses one of them at that size.
 FORWARD_DRAM_BYTES = 95.0e6
+FORWARD_DRAM_CONFIGS = (9, 10)
 
 
 def kernel_path(name: str, tmp: str) -> str:
@@ -75,6 +78,28 @@ def bench_image(size: int, seed: int, sigma: float):
 
     clean = lpaici.synth_image(size, size, seed)
     return clean, lpaici.add_noise(clean, sigma, SEED)
+
+
+def synth_module():
+    """lpaici/synth.py loaded on its own (numpy only): the reference arm builds the same image without
+    importing the package, whose import loads this project's library."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("lpaici_synth", os.path.join(PKG, "lpaici", "synth.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def reference_bench_image(size: int, seed: int, sigma: float):
+    """The benchmark image of bench_image, noise drawn by the reference's own create_noisy_image
+    (src/v1_0_lpa_ici_2D_fused.cpp:759-776, compiled into oracle/_ref/): bit-identical to lpaici.add_noise
+    (same std::mt19937 and std::normal_distribution<float>)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_bind as ob
+
+    clean = synth_module().synth_image(size, size, seed)
+    return clean, ob.ref_noise(clean, sigma, SEED)
 
 
 class Clocks:
@@ -260,6 +285,86 @@ class quiet_stdout:
         return False
 
 
+class capture_stdout(quiet_stdout):
+    """Like quiet_stdout, into a temporary file whose text is .text after the block."""
+
+    def __enter__(self):
+        import ctypes
+
+        self.libc = ctypes.CDLL(None)
+        sys.stdout.flush()
+        self.libc.fflush(None)
+        self.saved = os.dup(1)
+        self.file = tempfile.TemporaryFile(mode="w+b")
+        self.null = os.dup(self.file.fileno())
+        os.dup2(self.null, 1)
+        return self
+
+    def __exit__(self, *exc):
+        super().__exit__(*exc)
+        self.file.seek(0)
+        self.text = self.file.read().decode(errors="replace")
+        self.file.close()
+        return False
+
+
+def reference_gpu_v4_1(clean: np.ndarray, noisy: np.ndarray, ours: np.ndarray, steps: int) -> dict:
+    """The reference's own fastest GPU engine, anisotropic_lpa_ici_gpu_fused of
+    src/v4_1_lpa_ici_2D_sparse_shared.cu (:1122-1244: 16 launches of process_direction_fused_kernel +
+    aggregation, kernels in constant memory), compiled from its sources for sm_100a into
+    oracle/_ref/libref_v4_1.so and called as its main() does, on this run's image and GPU.  Timed by its
+    own window (after the uploads to after the download of the result, :1216-1240), read from the line it
+    prints, and by the wall clock of the whole call.  Its output is compared with this project's, which
+    is bit-exact with the reference's CPU engine: the v4_1 build lets nvcc contract its multiply-adds
+    into FFMA (default -fmad=true), so it differs where rounding moves an ICI decision."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_bind as ob
+
+    if not (ob.ref_available("v4_1") and ob.ref_available("v1_0")):
+        return {"unavailable": "oracle/_ref/libref_v4_1.so or libref_v1_0.so not built"}
+    tmp = tempfile.mkdtemp()
+    try:
+        with quiet_stdout():
+            k = ob.ref_load_kernels(kernel_path(SYM, tmp))
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    var = ob.ref_variances(k, np.float32(SIGMA))
+    H, W = noisy.shape
+    x = np.ascontiguousarray(noisy, np.float32)
+    out = np.zeros_like(x)
+    lib = ob.ref_lib("v4_1")
+    windows, walls = [], []
+    for i in range(1 + steps):  # the first call (module load, constant uploads) is not kept
+        with capture_stdout() as cap:
+            t0 = time.perf_counter()
+            lib.ref_gpu_fused(x, out, W, H, k.w, k.w.size, k.off, k.rows, k.cols, k.D, k.S, var, np.float32(GAMMA))
+            wall = time.perf_counter() - t0
+        t = [float(ln.rsplit(":", 1)[1].split()[0]) for ln in cap.text.splitlines()
+             if ln.startswith("Time taken for directional loops + aggregation")]
+        if i > 0 and t:
+            windows.append(t[-1])
+            walls.append(wall)
+    if not windows:
+        return {"unavailable": "the reference engine printed no timing line"}
+    px = W * H
+    a64, b64 = ours.astype(np.float64), out.astype(np.float64)
+    with quiet_stdout():
+        psnr_ours = ob.ref_psnr(clean, ours)
+        psnr_ref = ob.ref_psnr(clean, out)
+    return {"engine": "anisotropic_lpa_ici_gpu_fused, src/v4_1_lpa_ici_2D_sparse_shared.cu (built -O3 for sm_100a)",
+            "size": W, "steps": len(windows), "unit": UNIT,
+            "value": px / float(np.mean(windows)) / 1e6,
+            "window": "the reference's own: after the uploads to after the download of the result",
+            "value_wall": px / float(np.mean(walls)) / 1e6,
+            "ms_window": float(np.mean(windows)) * 1e3, "ms_wall": float(np.mean(walls)) * 1e3,
+            "ours_e2e_over_reference": None,
+            "output_vs_ours": {"max_abs_err": float(np.abs(a64 - b64).max()),
+                               "pixels_differing": int(np.count_nonzero(ours.view(np.uint32) != out.view(np.uint32))),
+                               "pixels_over_1e-4": int(np.count_nonzero(np.abs(a64 - b64) > 1e-4)),
+                               "psnr_ours_db": psnr_ours, "psnr_reference_gpu_db": psnr_ref,
+                               "psnr_delta_db": psnr_ref - psnr_ours}}
+
+
 def host_threads() -> int:
     try:
         return len(os.sched_getaffinity(0))
@@ -271,7 +376,7 @@ def run_reference(args, rank: int, world: int) -> None:
     if rank != 0:
         return
     threads = host_threads()
-    _, noisy = bench_image(SIZE, SEED, SIGMA)
+    _, noisy = reference_bench_image(SIZE, SEED, SIGMA)
     for _ in range(args.warmup):
         cpu_reference_sample(noisy, 64, threads, SIGMA, GAMMA, seed=1)
     vals, secs = [], []
@@ -286,7 +391,9 @@ def run_reference(args, rank: int, world: int) -> None:
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(secs)) * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "plain LPA-ICI forward, 4096x4096 synthetic, sym 16x7, sigma 20/255, gamma 2",
+        "config": {"workload": f"plain LPA-ICI forward, sym 16x7, sigma 20/255, gamma 2: a sample of {threads} crops "
+                               f"of {args.ref_crop}x{args.ref_crop} px of the 4096x4096 synthetic benchmark image per "
+                               "step, each denoised as a whole image",
                    "reference": "titocapovilla/lpa-ici-cuda src/v1_0_lpa_ici_2D_fused.cpp (CPU, built -O3)"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -383,6 +490,11 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         plan.close()
         extra["batched_one_image"] = {"size": size, "value": px / (np.mean(b_ms) * 1e-3) / 1e6,
                                       "plain": value, "unit": UNIT, "graph": True, "bit_equal_to_plain": bool(same)}
+        ref_gpu = reference_gpu_v4_1(clean, noisy_h, out.cpu().numpy(), min(args.steps, 3))
+        if "value" in ref_gpu:
+            ref_gpu["ours_e2e_over_reference"] = (px / e2e_step / 1e6) / ref_gpu["value"]
+            ref_gpu["ours_device_over_reference"] = value / ref_gpu["value"]
+        extra["reference_gpu_v4_1"] = ref_gpu
 
     cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -402,9 +514,14 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
             torch.distributed.barrier()
         return
     kernel_s = ms_step * 1e-3
-    peak_ops = max(peak["muladd_ops_per_s"], peak["prodadd2_ops_per_s"])  # the exact forms only
+    exact_ops = max(peak["muladd_ops_per_s"], peak["prodadd2_ops_per_s"])  # the exact forms only
+    ffma_flops = peak["ffma_ops_per_s"]  # the FP32 FMA pipe: 2 FLOP per FFMA
     achieved = 2.0 * taps / kernel_s  # one multiply + one add per tap
     tw, th, thr, ppt = lpaici.tile_configs()[best]
+    traffic = FORWARD_DRAM_BYTES if (size == SIZE and best in FORWARD_DRAM_CONFIGS) else None
+    traffic_note = ("bytes per launch, dram__bytes_read.sum + dram__bytes_write.sum: a constant from the ncu capture "
+                    "in profiles/forward_4096_sym.md (67.8 MB read + 27.2 MB written; algorithmic 134.2 MB: 4 B in "
+                    "+ 4 B out per pixel), not measured by this run")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -415,14 +532,18 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
                    "l2": "flushed between timed steps (256 MB write)",
                    "tile": {"config": best, "tile_w": tw, "tile_h": th, "threads": thr, "pixels_per_thread": ppt},
                    "parallelism": f"dp{world} (independent images, no collective)"},
-        "roofline": {"bound": "fp32", "achieved": achieved / 1e12, "peak": peak_ops / 1e12, "unit": "TFLOP/s",
-                     "frac": achieved / peak_ops, "traffic": FORWARD_DRAM_BYTES if size == SIZE else None,
-                     "traffic_note": "bytes per launch, dram__bytes_read.sum + dram__bytes_write.sum of one ncu "
-                                     "capture of this workload (67.8 MB read + 27.2 MB written; algorithmic "
-                                     "134.2 MB: 4 B in + 4 B out per pixel)",
-                     "note": "FLOP = 2 per algorithmic tap (multiply and add, each rounded: bit-exact with the "
-                             "reference); peak = the faster of the two exact FP32 forms measured live on this GPU "
-                             "(scalar FMUL+FADD, packed fma(w,x,-0)+add); scalar FFMA shown for context",
+        "roofline": {"bound": "fp32", "achieved": achieved / 1e12, "peak": ffma_flops / 1e12, "unit": "TFLOP/s",
+                     "frac": achieved / ffma_flops,
+                     "frac_exact_form": achieved / exact_ops, "peak_exact_form": exact_ops / 1e12,
+                     "traffic": traffic,
+                     "traffic_note": (traffic_note if traffic is not None else
+                                      f"null: the ncu figure is for tile configurations {FORWARD_DRAM_CONFIGS} at "
+                                      f"{SIZE}^2, this run used configuration {best} at {size}^2"),
+                     "note": "FLOP = 2 per algorithmic tap (one multiply and one add); peak = the FP32 FMA pipe "
+                             "(scalar FFMA chains, measured live on this GPU, 2 FLOP per FFMA).  The kernel keeps "
+                             "every product and sum separately rounded (bit-exact with the reference), so it cannot "
+                             "use FFMA: frac_exact_form divides by the exact forms' measured peak (the faster of "
+                             "scalar FMUL+FADD and packed fma(w,x,-0)+add), which is half the FFMA peak",
                      "algorithmic_taps_per_px": taps / px,
                      "fp32_probe_tops": {k: v / 1e12 for k, v in peak.items()}},
         "cpu_baseline": cpu,
@@ -443,15 +564,16 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
 def run_extras(torch, lpaici, ks, args, flush) -> dict:
     import concurrent.futures as cf
 
-    rng = np.random.default_rng(SEED)
-    n = 64
-    dims = rng.integers(256, 2049, size=(n, 2))
-    sig = (rng.uniform(10, 40, n).astype(np.float32) / np.float32(255.0)).astype(np.float32)
-    gam = rng.uniform(1.5, 2.5, n).astype(np.float32)
+    from lpaici.synth import mixed_batch
+
+    spec = mixed_batch(64, SEED)
+    n = len(spec)
+    sig = [s[2] for s in spec]
+    gam = [s[3] for s in spec]
 
     def make(i):
-        w, h = int(dims[i, 0]), int(dims[i, 1])
-        return lpaici.add_noise(lpaici.synth_image(w, h, SEED + 1 + i), float(sig[i]), SEED + i)
+        w, h, s, _, img_seed, noise_seed = spec[i]
+        return lpaici.add_noise(lpaici.synth_image(w, h, img_seed), s, noise_seed)
 
     with cf.ThreadPoolExecutor(max_workers=min(16, host_threads())) as ex:
         hosts = list(ex.map(make, range(n)))

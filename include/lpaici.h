@@ -260,8 +260,11 @@ int lpaici_trim_workspace(void);
  *     LPAICI_ERR_UNSUPPORTED before any CUDA call.
  *   - Nothing has to start at zero: every call copies the blobs in (host to device on `stream`) and
  *     the selection sweep writes every byte the gather reads.
- *   - The first call on each device looks up the array's address with cudaGetSymbolAddress, which
- *     can load the module holding it; a caller that captures streams makes that first call before.
+ *   - Every call looks up the array's address with cudaGetSymbolAddress; the first call on a device
+ *     can load the module holding it, so a caller that captures streams makes that first call before.
+ *   - Under CUDA's default lazy module loading, the 64 MiB are reserved on a device only once a process
+ *     calls this entry point there; with CUDA_MODULE_LOADING=EAGER every process that loads the
+ *     library reserves them on every device it uses, forward-only and command-line users included.
  *   - One scratch per device: calls that overlap on one device (different streams or threads with
  *     work in flight at once) race on it.  Serialise them, e.g. on one stream. */
 int lpaici_backward_noalloc(const lpaici_kernelset *ks, const float *d_noisy, int noisy_pitch,

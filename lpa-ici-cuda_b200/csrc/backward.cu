@@ -16,6 +16,7 @@
 //      deterministic.
 // No counterpart in the reference.
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <mutex>
 #include <vector>
@@ -477,6 +478,15 @@ int workspace_pool(cudaMemPool_t *out) {
 
 }  // namespace
 
+int check_adjoint_params(const lpaici_kernelset *ks, float sigma, const float *gamma, const char *who) {
+    if (!(sigma > 0.0f) || !std::isfinite(sigma) || (gamma && (!(*gamma > 0.0f) || !std::isfinite(*gamma))))
+        return set_error(LPAICI_ERR_INVALID_ARG, "%s: sigma and gamma need finite positive numbers", who);
+    if (ks->S > kMaxScales)
+        return set_error(LPAICI_ERR_UNSUPPORTED, "%s: %d scales per direction; the adjoint supports at most %d", who,
+                         ks->S, kMaxScales);
+    return LPAICI_OK;
+}
+
 }  // namespace lpaici
 
 using namespace lpaici;
@@ -502,12 +512,11 @@ extern "C" int lpaici_backward(const lpaici_kernelset *ks, const float *d_noisy,
         return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_backward: null argument");
     if (width <= 0 || height <= 0 || noisy_pitch < width || gout_pitch < width || gin_pitch < width)
         return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_backward: bad size or pitch");
-    if (!(sigma > 0.0f) || !(gamma > 0.0f))
-        return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_backward: sigma and gamma need positive numbers");
-    if (ks->S > 32) return set_error(LPAICI_ERR_UNSUPPORTED, "lpaici_backward supports at most 32 scales");
+    int rc = check_adjoint_params(ks, sigma, &gamma, "lpaici_backward");
+    if (rc != LPAICI_OK) return rc;
     cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
     const int *blob = nullptr, *adj = nullptr;
-    int rc = device_blob(ks, &blob);
+    rc = device_blob(ks, &blob);
     if (rc == LPAICI_OK) rc = device_adj_blob(ks, &adj);
     if (rc != LPAICI_OK) return rc;
 
@@ -572,15 +581,13 @@ extern "C" int lpaici_backward_batch_create(const lpaici_kernelset *ks, const lp
     if (!ks || !images || n <= 0 || !out)
         return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_backward_batch_create: bad argument");
     *out = nullptr;
-    if (ks->S > 32) return set_error(LPAICI_ERR_UNSUPPORTED, "the adjoint supports at most 32 scales");
     for (int i = 0; i < n; i++) {
         const lpaici_grad_image &im = images[i];
         if (!im.noisy || !im.grad_out || !im.grad_in || im.width <= 0 || im.height <= 0 || im.noisy_pitch < im.width ||
             im.gout_pitch < im.width || im.gin_pitch < im.width)
             return set_error(LPAICI_ERR_INVALID_ARG, "adjoint batch image %d: bad pointer, size or pitch", i);
-        if (!(im.sigma > 0.0f) || !(im.gamma > 0.0f))
-            return set_error(LPAICI_ERR_INVALID_ARG, "adjoint batch image %d: sigma and gamma need positive numbers",
-                             i);
+        const int rc = check_adjoint_params(ks, im.sigma, &im.gamma, "lpaici_backward_batch_create");
+        if (rc != LPAICI_OK) return rc;
     }
     cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
     const int *adj = nullptr;
@@ -740,9 +747,7 @@ size_t state_smap_bytes(const lpaici_kernelset *ks, int width, int height) {
 int state_args(const lpaici_kernelset *ks, int width, int height, float sigma, const char *who) {
     if (!ks) return set_error(LPAICI_ERR_INVALID_ARG, "%s: null kernel set", who);
     if (width <= 0 || height <= 0) return set_error(LPAICI_ERR_INVALID_ARG, "%s: bad size %d x %d", who, width, height);
-    if (!(sigma > 0.0f)) return set_error(LPAICI_ERR_INVALID_ARG, "%s: sigma needs a positive number", who);
-    if (ks->S > 32) return set_error(LPAICI_ERR_UNSUPPORTED, "%s: the adjoint supports at most 32 scales", who);
-    return LPAICI_OK;
+    return check_adjoint_params(ks, sigma, nullptr, who);
 }
 
 }  // namespace
@@ -759,7 +764,8 @@ extern "C" int lpaici_forward_state(const lpaici_kernelset *ks, const float *d_n
     if (rc != LPAICI_OK) return rc;
     if (!d_noisy || !d_denoised || !d_state || noisy_pitch < width || out_pitch < width)
         return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_forward_state: null pointer or bad pitch");
-    if (!(gamma > 0.0f)) return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_forward_state: gamma needs a positive number");
+    rc = check_adjoint_params(ks, sigma, &gamma, "lpaici_forward_state");
+    if (rc != LPAICI_OK) return rc;
     const int *blob = nullptr;
     rc = device_blob(ks, &blob);
     if (rc != LPAICI_OK) return rc;

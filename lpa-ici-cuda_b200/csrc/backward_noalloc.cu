@@ -7,9 +7,10 @@
 // Nothing in it needs to start at zero: the two blobs are copied in by every call, pass A writes every
 // selection byte and 1/den value that pass B reads.
 //
-// The array lives in its own translation unit, so the module that holds it is loaded only by callers of
-// this entry point.  No counterpart in the reference.
-#include <mutex>
+// The array lives in its own translation unit.  Under CUDA's default lazy module loading the module that
+// holds it is loaded, and its 64 MiB reserved on a device, only when a process calls this entry point on
+// that device; with CUDA_MODULE_LOADING=EAGER every process that loads the library reserves it on every
+// device it uses.  No counterpart in the reference.
 
 #include "internal.h"
 
@@ -20,28 +21,17 @@ namespace {
 constexpr size_t kScratchBytes = LPAICI_NOALLOC_SCRATCH_BYTES;
 __device__ __align__(256) unsigned char g_adjoint_scratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_lock;
-void *g_scratch_address[kMaxDevices];  // per device, looked up once
-
 size_t round256(size_t n) { return (n + 255) & ~size_t(255); }
 
-// Address of the scratch array on the current device: cudaGetSymbolAddress on the first call per
-// device (this can load the module holding the array), cached afterwards.
+// Address of the scratch array on the current device.  Looked up on every call (cheap once the module
+// is loaded): after a cudaDeviceReset the module is loaded again, possibly at another address.  In host
+// code g_adjoint_scratch names a host-side stand-in, never a device address.  The first call on a
+// device can load the module holding the array.
 int scratch_address(unsigned char **out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return cuda_error(e, "cudaGetDevice");
-    if (dev < 0 || dev >= kMaxDevices)
-        return set_error(LPAICI_ERR_UNSUPPORTED, "lpaici_backward_noalloc: device %d beyond %d", dev, kMaxDevices);
-    std::lock_guard<std::mutex> hold(g_lock);
-    if (!g_scratch_address[dev]) {
-        void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_adjoint_scratch);
-        if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress(adjoint scratch)");
-        g_scratch_address[dev] = p;
-    }
-    *out = static_cast<unsigned char *>(g_scratch_address[dev]);
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_adjoint_scratch);
+    if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress(adjoint scratch)");
+    *out = static_cast<unsigned char *>(p);
     return LPAICI_OK;
 }
 
@@ -54,9 +44,8 @@ extern "C" int lpaici_backward_noalloc(const lpaici_kernelset *ks, const float *
         return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_backward_noalloc: null argument");
     if (width <= 0 || height <= 0 || noisy_pitch < width || gout_pitch < width || gin_pitch < width)
         return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_backward_noalloc: bad size or pitch");
-    if (!(sigma > 0.0f) || !(gamma > 0.0f))
-        return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_backward_noalloc: sigma and gamma need positive numbers");
-    if (ks->S > 32) return set_error(LPAICI_ERR_UNSUPPORTED, "lpaici_backward_noalloc supports at most 32 scales");
+    const int prc = check_adjoint_params(ks, sigma, &gamma, "lpaici_backward_noalloc");
+    if (prc != LPAICI_OK) return prc;
 
     // sizes are checked before any CUDA call
     const size_t npx = static_cast<size_t>(width) * height;

@@ -59,6 +59,10 @@ struct KernelTables {
 
 int set_error(int code, const char *fmt, ...);
 int cuda_error(cudaError_t e, const char *what);
+// The checks every adjoint entry point makes before any copy or launch: sigma and gamma finite and
+// positive (gamma only when the caller passes one), at most kMaxScales scales per direction (the
+// selection sweep keeps each pixel's scale in 4 bits).  `who` names the entry point in the message.
+int check_adjoint_params(const lpaici_kernelset *ks, float sigma, const float *gamma, const char *who);
 
 }  // namespace lpaici
 

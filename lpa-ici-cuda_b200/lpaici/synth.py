@@ -85,3 +85,16 @@ def synth_image(width: int, height: int, seed: int, rgbe: bool = True) -> np.nda
             patch[m] = level
     np.clip(img, 0.0, 1.0, out=img)
     return rgbe_quantize(img) if rgbe else img
+
+
+def mixed_batch(n: int = 64, seed: int = 20250910):
+    """The mixed batch of the batched benchmark: n images with width and height drawn uniformly from
+    256..2048, sigma uniform in 10/255..40/255 and gamma uniform in 1.5..2.5 (FP32), all from one
+    generator seeded with `seed`.  Returns (width, height, sigma, gamma, image_seed, noise_seed) per
+    image: image i is synth_image(width, height, seed + 1 + i) with noise seed seed + i."""
+    rng = np.random.default_rng(seed)
+    dims = rng.integers(256, 2049, size=(n, 2))
+    sig = (rng.uniform(10, 40, n).astype(np.float32) / np.float32(255.0)).astype(np.float32)
+    gam = rng.uniform(1.5, 2.5, n).astype(np.float32)
+    return [(int(dims[i, 0]), int(dims[i, 1]), float(sig[i]), float(gam[i]), seed + 1 + i, seed + i)
+            for i in range(n)]

@@ -13,7 +13,23 @@ for p in (PKG, TESTS):
         sys.path.insert(0, p)
 
 GOLDEN = os.path.join(TESTS, "golden")
-REFERENCE_KERNELS = "/root/reference/kernels"
+
+
+def _reference_root():
+    """Root of the reference project: LPAICI_REFERENCE, else the tree oracle/_ref/ was built from
+    (recorded by oracle/Makefile); None when neither names an existing directory."""
+    root = os.environ.get("LPAICI_REFERENCE")
+    if not root:
+        rec = os.path.join(ROOT, "oracle", "_ref", "reference_root")
+        if os.path.exists(rec):
+            with open(rec) as f:
+                root = f.read().strip()
+    return root if root and os.path.isdir(root) else None
+
+
+REFERENCE_ROOT = _reference_root()
+# the reference's kernel files (kernels/*.txt); a path that does not exist when the tree is absent
+REFERENCE_KERNELS = os.path.join(REFERENCE_ROOT, "kernels") if REFERENCE_ROOT else os.path.join(ROOT, "_no_reference")
 SYM = "lpa_kernels_m_1_0_d_16_h12_1_2_4_8_16_24_32_symmetric.txt"
 GAUSS_M2 = "lpa_kernels_m_2_0_d_16_h12_1_2_4_8_16_24_32_gaussian.txt"
 SMALL = "lpa_kernels_m_1_0_d_8_h12_1_2_4_8.txt"

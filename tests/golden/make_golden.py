@@ -1,6 +1,6 @@
 """Generates the committed fixtures of tests/golden/ from the reference itself.
 
-Run in a container where the reference tree exists (default /root/reference) and oracle/_ref/ is built
+Run where the reference tree exists (--reference, default $LPAICI_REFERENCE) and oracle/_ref/ is built
 (`make -C oracle`).  Everything here comes out of the reference's own code, called in-process:
   kernels/*.txt.gz         copies of four of the reference's kernel files (inputs of the path)
   barbara_gray_u8.npy      data/barbara.png as stbi_load(.., 1) returns it (8-bit gray, before the
@@ -11,7 +11,7 @@ Run in a container where the reference tree exists (default /root/reference) and
                            (compute_kernel_variances) and the denoised image of
                            anisotropic_lpa_ici_cpu_fused (src/v1_0_lpa_ici_2D_fused.cpp:851-930)
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py [--reference <reference root>]   (default: $LPAICI_REFERENCE)
 """
 import argparse
 import gzip
@@ -57,7 +57,7 @@ CASES = {
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("LPAICI_REFERENCE"), required="LPAICI_REFERENCE" not in os.environ)
     args = ap.parse_args()
     kdir = os.path.join(HERE, "kernels")
     os.makedirs(kdir, exist_ok=True)

@@ -3,7 +3,7 @@ by the reference's own loader (load_LPA_kernels_standardized, compiled in-proces
 oracle/_ref/) and stored as this library's binary tap-list file (lpaici_kernelset_save), so that the GPU
 tests can run every kernel set without the reference tree.
 
-    python tests/golden/make_kernel_taps.py [--reference /root/reference]
+    python tests/golden/make_kernel_taps.py [--reference <reference root>]   (default: $LPAICI_REFERENCE)
 """
 import argparse
 import glob
@@ -19,7 +19,7 @@ import lpaici  # noqa: E402
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("LPAICI_REFERENCE"), required="LPAICI_REFERENCE" not in os.environ)
     args = ap.parse_args()
     out_dir = os.path.join(HERE, "kernels", "taps")
     os.makedirs(out_dir, exist_ok=True)

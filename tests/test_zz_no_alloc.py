@@ -90,6 +90,82 @@ def test_noalloc_pitched_buffers_and_repeat():
     assert np.isnan(op[:, W:].cpu().numpy()).all()  # nothing written outside the gradient's columns
 
 
+def _r256(n: int) -> int:
+    return (n + 255) & ~255
+
+
+def _scratch_need(ks, W: int, H: int) -> int:
+    """Bytes lpaici_backward_noalloc needs: the layout of kernelset.cpp's two device blobs (int words:
+    run ranges padded to 4, 4 per run, then {w, w} per tap with runs padded to even length and 16 spare
+    taps / one float per tap and 16 spare), each 256-rounded, then D*W*H selection bytes (256-rounded)
+    and W*H floats of 1/den."""
+    r = ks.runs()
+    nk = ks.D * ks.S
+    head = (nk + 1 + 3) & ~3
+    run_words = 4 * len(r.run_len)
+    n2 = int(sum((int(n) + 1) & ~1 for n in r.run_len))
+    blob_words = (head + run_words + 2 * (n2 + 16) + 3) & ~3
+    adj_words = (head + run_words + int(r.run_len.sum()) + 16 + 3) & ~3
+    return _r256(4 * blob_words) + _r256(4 * adj_words) + _r256(ks.D * W * H) + 4 * W * H
+
+
+def _largest_rows(ks, W: int) -> int:
+    H = SCRATCH_BYTES // (ks.D + 4) // W
+    while _scratch_need(ks, W, H + 1) <= SCRATCH_BYTES:
+        H += 1
+    while _scratch_need(ks, W, H) > SCRATCH_BYTES:
+        H -= 1
+    return H
+
+
+def test_noalloc_size_limit_is_exact():
+    """The largest image the scratch holds is accepted and one more row is rejected, both before any
+    device work.  The rejected call never touches its (fake) pointers; the accepted one is made only
+    where no CUDA device is visible, so it stops at the first CUDA call."""
+    import torch
+
+    ks = lpaici.KernelSet.load(kernel_file(SYM))
+    lib = lpaici.lib()
+    fake = C.c_void_p(256)
+    W = 1920
+    H = _largest_rows(ks, W)
+    assert _scratch_need(ks, W, H) <= SCRATCH_BYTES < _scratch_need(ks, W, H + 1)
+    rc = lib.lpaici_backward_noalloc(ks.handle, fake, W, fake, W, fake, W, W, H + 1, SIGMA_20, 2.0, None)
+    assert rc == lpaici.ERR_UNSUPPORTED
+    assert f"needs {_scratch_need(ks, W, H + 1)} bytes" in lib.lpaici_last_error().decode()
+    if not torch.cuda.is_available():
+        rc = lib.lpaici_backward_noalloc(ks.handle, fake, W, fake, W, fake, W, W, H, SIGMA_20, 2.0, None)
+        assert rc != lpaici.OK and "needs" not in lib.lpaici_last_error().decode()
+
+
+def test_noalloc_rejects_bad_parameters_before_any_copy():
+    """Non-finite sigma or gamma and more scales than the selection sweep keeps are refused up front."""
+    ks = lpaici.KernelSet.load(kernel_file(SYM))
+    lib = lpaici.lib()
+    fake = C.c_void_p(256)
+    for sigma, gamma in ((float("inf"), 2.0), (SIGMA_20, float("inf")), (float("nan"), 2.0), (SIGMA_20, 0.0)):
+        rc = lib.lpaici_backward_noalloc(ks.handle, fake, 8, fake, 8, fake, 8, 8, 8, sigma, gamma, None)
+        assert rc == lpaici.ERR_INVALID_ARG, (sigma, gamma)
+        assert "finite positive" in lib.lpaici_last_error().decode()
+
+
+@pytest.mark.gpu
+def test_noalloc_at_the_size_limit():
+    """The largest accepted image (1920 columns): the blob offsets and the 1/den tail at the end of the
+    scratch are right, so the gradient equals lpaici_backward's."""
+    import torch
+
+    ks = lpaici.KernelSet.load(kernel_file(SYM))
+    W = 1920
+    H = _largest_rows(ks, W)
+    noisy, g, xt, gt = _inputs(W, H, SIGMA_20, 24)
+    out = torch.full((H, W), float("nan"), device="cuda")
+    got = _call("lpaici_backward_noalloc", ks, xt, gt, out, SIGMA_20, 2.0)
+    ref = _call("lpaici_backward", ks, xt, gt, torch.empty_like(xt), SIGMA_20, 2.0)
+    assert np.isfinite(got).all()
+    _close(got, ref)
+
+
 def test_noalloc_rejects_images_beyond_the_scratch():
     """Sizes are checked before any CUDA call, so this runs without a GPU: the pointers are never used."""
     ks = lpaici.KernelSet.load(kernel_file(SYM))
