@@ -1,4 +1,4 @@
-// image_io.cpp -- PNG / Radiance HDR / PGM reading and Radiance HDR writing for the command line.
+// image_io.cpp -- PNG / BMP / TGA / Radiance HDR / PGM reading and Radiance HDR writing for the command line.
 // Conversions follow what stb_image (v2.30) and stb_image_write (v1.16), the reference's vendored
 // image libraries, do on the same files; the code is this project's own.
 #include "image_io.h"
@@ -243,6 +243,231 @@ bool load_pgm(const std::vector<uint8_t> &f, std::vector<float> &img, int &W, in
     return true;
 }
 
+// 8-bit pixels with n = 1 (gray), 3 (RGB) or 4 (RGBA) channels, row-major top-down, to the float image
+// stbi_loadf returns with `comps` channels: gray is the integer luma of RGB (alpha ignored), RGB
+// replicates gray, and every 8-bit value goes through the LDR-to-float table.
+void ldr_to_image(const std::vector<uint8_t> &px, int n, int W, int H, int comps, std::vector<float> &img) {
+    const float *lut = ldr_to_float_table();
+    const size_t npx = static_cast<size_t>(W) * H;
+    img.resize(npx * comps);
+    for (size_t i = 0; i < npx; i++) {
+        const uint8_t *p = &px[i * n];
+        if (comps == 1) {
+            img[i] = lut[n == 1 ? p[0] : luma(p[0], p[1], p[2])];
+        } else {
+            for (int k = 0; k < 3; k++) img[i * 3 + k] = lut[n == 1 ? p[0] : p[k]];
+        }
+    }
+}
+
+inline uint32_t le16(const uint8_t *p) { return uint32_t(p[0]) | (uint32_t(p[1]) << 8); }
+inline uint32_t le32(const uint8_t *p) { return le16(p) | (le16(p + 2) << 16); }
+
+// An n-bit field (n = 1..8) widened to 8 bits by repeating its bits (n = 5: v << 3 | v >> 2), as stb
+// does for BMP channel masks.
+inline uint8_t widen_bits(uint32_t v, int n) {
+    if (n <= 0) return 0;
+    if (n >= 8) return static_cast<uint8_t>(v >> (n - 8));
+    uint32_t x = v << (8 - n);
+    for (int k = n; k < 8; k += n) x |= x >> n;
+    return static_cast<uint8_t>(x);
+}
+
+// Windows / OS2 BMP: 1, 4, 8 bits with a palette, 16/24/32 bits (BI_RGB or BI_BITFIELDS masks), bottom-up
+// or (negative height) top-down, rows padded to 4 bytes.  Compressed (RLE) files are refused, as stb
+// refuses them.
+bool load_bmp(const std::vector<uint8_t> &f, std::vector<float> &img, int &W, int &H, int comps, std::string &err) {
+    if (f.size() < 26) return err = "truncated BMP", false;
+    const uint32_t data_off = le32(&f[10]), hsz = le32(&f[14]);
+    if (hsz != 12 && hsz != 40 && hsz != 56 && hsz != 108 && hsz != 124) return err = "unsupported BMP header", false;
+    if (f.size() < 14 + static_cast<size_t>(hsz)) return err = "truncated BMP", false;
+    int w, h, bpp;
+    uint32_t compress = 0;
+    if (hsz == 12) {
+        w = static_cast<int16_t>(le16(&f[18]));
+        h = static_cast<int16_t>(le16(&f[20]));
+        bpp = le16(&f[24]);
+    } else {
+        w = static_cast<int32_t>(le32(&f[18]));
+        h = static_cast<int32_t>(le32(&f[22]));
+        bpp = le16(&f[28]);
+        compress = le32(&f[30]);
+    }
+    const bool flip = h > 0;  // stored bottom-up
+    if (h < 0) h = -h;
+    if (w <= 0 || h <= 0 || w > (1 << 24) || h > (1 << 24)) return err = "bad BMP size", false;
+    if (compress != 0 && !(compress == 3 && (bpp == 16 || bpp == 32))) return err = "unsupported BMP compression", false;
+    uint32_t mask[4] = {0, 0, 0, 0};
+    if (bpp == 16) {
+        mask[0] = 0x7c00;
+        mask[1] = 0x03e0;
+        mask[2] = 0x001f;
+    } else if (bpp == 32) {
+        mask[0] = 0xff0000;
+        mask[1] = 0xff00;
+        mask[2] = 0xff;
+        mask[3] = 0xff000000u;
+    }
+    if (compress == 3) {
+        const size_t mo = 14 + 40;  // after the 40-byte header, or inside a V4/V5 header
+        if (hsz == 12 || hsz == 56 || f.size() < mo + 12) return err = "unsupported BMP bitfields", false;
+        mask[0] = le32(&f[mo]);
+        mask[1] = le32(&f[mo + 4]);
+        mask[2] = le32(&f[mo + 8]);
+    }
+    std::vector<uint8_t> pal;
+    if (bpp <= 8) {
+        const int entry = hsz == 12 ? 3 : 4;
+        const size_t pal_off = 14 + hsz;
+        const size_t n = (data_off - pal_off) / entry;
+        if (data_off < pal_off || n == 0 || n > 256) return err = "bad BMP palette", false;
+        pal.assign(256 * 3, 0);
+        for (size_t i = 0; i < n; i++)
+            for (int k = 0; k < 3; k++) pal[i * 3 + k] = f[pal_off + i * entry + 2 - k];  // stored B, G, R
+    } else if (bpp != 16 && bpp != 24 && bpp != 32) {
+        return err = "unsupported BMP bit depth", false;
+    }
+    int shift[4], bits[4];
+    for (int c = 0; c < 4; c++) {
+        shift[c] = 0;
+        bits[c] = 0;
+        if (mask[c]) {
+            uint32_t m = mask[c];
+            while (!(m & 1u)) m >>= 1, shift[c]++;
+            while (m & 1u) m >>= 1, bits[c]++;
+        }
+    }
+    if (bpp == 16 || bpp == 32) {  // stb refuses missing colour masks and fields wider than 8 bits
+        if (!mask[0] || !mask[1] || !mask[2]) return err = "bad BMP masks", false;
+        for (int c = 0; c < 4; c++)
+            if (bits[c] > 8) return err = "bad BMP masks", false;
+    }
+    const size_t stride = ((static_cast<size_t>(w) * bpp + 31) / 32) * 4;
+    if (f.size() < data_off + stride * h) return err = "truncated BMP", false;
+    W = w;
+    H = h;
+    std::vector<uint8_t> px(static_cast<size_t>(w) * h * 3);
+    for (int y = 0; y < h; y++) {
+        const uint8_t *row = &f[data_off + stride * (flip ? h - 1 - y : y)];
+        uint8_t *dst = &px[static_cast<size_t>(y) * w * 3];
+        for (int x = 0; x < w; x++, dst += 3) {
+            if (bpp <= 8) {
+                const int per = 8 / bpp, b = x / per, k = per - 1 - x % per;
+                const int idx = (row[b] >> (k * bpp)) & ((1 << bpp) - 1);
+                std::memcpy(dst, &pal[idx * 3], 3);
+            } else if (bpp == 24) {
+                dst[0] = row[3 * x + 2];
+                dst[1] = row[3 * x + 1];
+                dst[2] = row[3 * x];
+            } else {
+                const uint32_t v = bpp == 16 ? le16(row + 2 * x) : le32(row + 4 * x);
+                for (int c = 0; c < 3; c++) dst[c] = widen_bits((v & mask[c]) >> shift[c], bits[c]);
+            }
+        }
+    }
+    ldr_to_image(px, 3, w, h, comps, img);
+    return true;
+}
+
+// Truevision TGA: color-mapped (1, 9), truecolor (2, 10) and gray (3, 11) images, raw or run-length;
+// 8/15/16/24/32 bits; bottom-up unless the descriptor's top-left bit is set.  15/16-bit pixels are
+// 5-5-5 with each field scaled as v * 255 / 31 (stb's TGA reader).
+bool load_tga(const std::vector<uint8_t> &f, std::vector<float> &img, int &W, int &H, int comps, std::string &err) {
+    if (f.size() < 18) return err = "truncated TGA", false;
+    const int id_len = f[0], cmap_type = f[1], type = f[2];
+    const int cmap_first = le16(&f[3]), cmap_len = le16(&f[5]), cmap_bits = f[7];
+    const int w = le16(&f[12]), h = le16(&f[14]), bpp = f[16], desc = f[17];
+    const bool rle = type >= 9;
+    const int base = rle ? type - 8 : type;
+    if ((base != 1 && base != 2 && base != 3) || w <= 0 || h <= 0) return err = "unsupported TGA", false;
+    if (base == 1 && (cmap_type != 1 || (bpp != 8 && bpp != 16))) return err = "unsupported TGA palette", false;
+    if (base == 3 && bpp != 8 && bpp != 16) return err = "unsupported TGA gray depth", false;
+    if (base == 2 && bpp != 15 && bpp != 16 && bpp != 24 && bpp != 32) return err = "unsupported TGA depth", false;
+    size_t pos = 18 + id_len;
+    // color map entries as RGB
+    std::vector<uint8_t> cmap;
+    auto color = [&](const uint8_t *p, int bits, uint8_t *rgb) {
+        if (bits == 15 || bits == 16) {
+            const uint32_t v = le16(p);
+            rgb[0] = static_cast<uint8_t>((((v >> 10) & 31) * 255) / 31);
+            rgb[1] = static_cast<uint8_t>((((v >> 5) & 31) * 255) / 31);
+            rgb[2] = static_cast<uint8_t>(((v & 31) * 255) / 31);
+        } else {  // 24 / 32: B, G, R (, A)
+            rgb[0] = p[2];
+            rgb[1] = p[1];
+            rgb[2] = p[0];
+        }
+    };
+    if (cmap_type == 1) {
+        // as stb reads it: the first-entry field is a count of bytes skipped before the map, and pixel
+        // indexes address the map directly (an index past its end reads entry 0)
+        const int eb = (cmap_bits + 7) / 8;
+        if (base == 1) pos += cmap_first;
+        if (f.size() < pos + static_cast<size_t>(cmap_len) * eb) return err = "truncated TGA", false;
+        if (base == 1) {
+            if (cmap_len == 0 || (cmap_bits != 15 && cmap_bits != 16 && cmap_bits != 24 && cmap_bits != 32))
+                return err = "unsupported TGA palette", false;
+            cmap.assign(static_cast<size_t>(cmap_len) * 3, 0);
+            for (int i = 0; i < cmap_len; i++) color(&f[pos + static_cast<size_t>(i) * eb], cmap_bits, &cmap[i * 3]);
+        }
+        pos += static_cast<size_t>(cmap_len) * eb;
+    }
+    const int n = base == 3 ? 1 : 3;
+    const int pb = (bpp + 7) / 8;
+    W = w;
+    H = h;
+    std::vector<uint8_t> px(static_cast<size_t>(w) * h * n);
+    auto put = [&](size_t i, const uint8_t *p) -> bool {
+        uint8_t *dst = &px[i * n];
+        if (base == 3) {
+            dst[0] = p[0];  // 16-bit gray: the low byte is the gray value (the high byte is alpha)
+        } else if (base == 1) {
+            int idx = bpp == 8 ? p[0] : static_cast<int>(le16(p));
+            if (idx >= cmap_len) idx = 0;
+            std::memcpy(dst, &cmap[static_cast<size_t>(idx) * 3], 3);
+        } else {
+            color(p, bpp, dst);
+        }
+        return true;
+    };
+    const size_t npx = static_cast<size_t>(w) * h;
+    size_t i = 0;
+    while (i < npx) {
+        if (!rle) {
+            if (pos + pb > f.size()) return err = "truncated TGA", false;
+            if (!put(i++, &f[pos])) return err = "bad TGA color index", false;
+            pos += pb;
+            continue;
+        }
+        if (pos >= f.size()) return err = "truncated TGA", false;
+        const int hdr = f[pos++], count = (hdr & 127) + 1;
+        if (hdr & 128) {
+            if (pos + pb > f.size()) return err = "truncated TGA", false;
+            for (int k = 0; k < count && i < npx; k++)
+                if (!put(i++, &f[pos])) return err = "bad TGA color index", false;
+            pos += pb;
+        } else {
+            for (int k = 0; k < count && i < npx; k++) {
+                if (pos + pb > f.size()) return err = "truncated TGA", false;
+                if (!put(i++, &f[pos])) return err = "bad TGA color index", false;
+                pos += pb;
+            }
+        }
+    }
+    if (!(desc & 32)) {  // bottom-up: flip rows
+        const size_t rb = static_cast<size_t>(w) * n;
+        std::vector<uint8_t> tmp(rb);
+        for (int y = 0; y < h / 2; y++) {
+            uint8_t *a = &px[y * rb], *b = &px[(h - 1 - y) * rb];
+            std::memcpy(tmp.data(), a, rb);
+            std::memcpy(a, b, rb);
+            std::memcpy(b, tmp.data(), rb);
+        }
+    }
+    ldr_to_image(px, n, w, h, comps, img);
+    return true;
+}
+
 // RGBE pixel to gray: (R + G + B) * 2^(E - 136) / 3 in float, 0 when E == 0; to RGB: each
 // mantissa byte times 2^(E - 136).
 inline float rgbe_gray(const uint8_t *p) {
@@ -392,7 +617,11 @@ bool load_image(const std::string &path, int comps, std::vector<float> &img, int
     if (f.size() >= 8 && !std::memcmp(f.data(), png_sig, 8)) return load_png(f, img, width, height, comps, err);
     if (f.size() >= 2 && f[0] == '#' && f[1] == '?') return load_hdr(f, img, width, height, comps, err);
     if (f.size() >= 2 && f[0] == 'P' && f[1] == '5') return load_pgm(f, img, width, height, comps, err);
-    return err = "unsupported image format (PNG, Radiance HDR and binary PGM are read)", false;
+    if (f.size() >= 2 && f[0] == 'B' && f[1] == 'M') return load_bmp(f, img, width, height, comps, err);
+    // TGA has no signature: tried last, on its header's plausibility (as stb tries it last)
+    if (f.size() >= 18 && (f[1] == 0 || f[1] == 1) && ((f[2] >= 1 && f[2] <= 3) || (f[2] >= 9 && f[2] <= 11)))
+        return load_tga(f, img, width, height, comps, err);
+    return err = "unsupported image format (PNG, BMP, TGA, Radiance HDR and binary PGM are read)", false;
 }
 
 bool load_gray(const std::string &path, std::vector<float> &img, int &width, int &height, std::string &err) {

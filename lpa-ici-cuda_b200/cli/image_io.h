@@ -6,7 +6,10 @@
 //     not): 16-bit samples keep their high byte, RGB becomes (77 R + 150 G + 29 B) >> 8, then every
 //     8-bit value v becomes (float) pow(v / 255.0f, 2.2f) -- stb's LDR-to-HDR conversion;
 //   * Radiance .hdr (RGBE, flat or run-length scanlines): gray = (R + G + B) * 2^(E - 136) / 3;
-//   * binary PGM (P5, 8-bit), converted like 8-bit PNG gray.
+//   * binary PGM (P5, 8-bit), converted like 8-bit PNG gray;
+//   * BMP (1/4/8-bit palettes, 16/32-bit bit fields of up to 8 bits, 24/32-bit; bottom-up or top-down; no
+//     RLE) and TGA (color-mapped, truecolor 15/16/24/32-bit, gray 8/16-bit; raw or run-length), as
+//     stb reads them, then converted like 8-bit PNG.
 // Writing produces a Radiance .hdr (RGBE, run-length scanlines for widths 8..32767), gray stored as
 // R = G = B, as stbi_write_hdr does for one channel (src/v4_1_lpa_ici_2D_sparse_shared.cu:388, :522).
 #pragma once
