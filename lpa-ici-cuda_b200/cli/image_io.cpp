@@ -1,4 +1,4 @@
-// image_io.cpp -- PNG / BMP / TGA / Radiance HDR / PGM reading and Radiance HDR writing for the command line.
+// image_io.cpp -- PNG / JPEG / BMP / TGA / Radiance HDR / PGM reading and Radiance HDR writing for the command line.
 // Conversions follow what stb_image (v2.30) and stb_image_write (v1.16), the reference's vendored
 // image libraries, do on the same files; the code is this project's own.
 #include "image_io.h"
@@ -618,10 +618,16 @@ bool load_image(const std::string &path, int comps, std::vector<float> &img, int
     if (f.size() >= 2 && f[0] == '#' && f[1] == '?') return load_hdr(f, img, width, height, comps, err);
     if (f.size() >= 2 && f[0] == 'P' && f[1] == '5') return load_pgm(f, img, width, height, comps, err);
     if (f.size() >= 2 && f[0] == 'B' && f[1] == 'M') return load_bmp(f, img, width, height, comps, err);
+    if (f.size() >= 3 && f[0] == 0xff && f[1] == 0xd8 && f[2] == 0xff) {
+        std::vector<uint8_t> px;
+        if (!decode_jpeg(f, comps, px, width, height, err)) return false;
+        ldr_to_image(px, comps, width, height, comps, img);
+        return true;
+    }
     // TGA has no signature: tried last, on its header's plausibility (as stb tries it last)
     if (f.size() >= 18 && (f[1] == 0 || f[1] == 1) && ((f[2] >= 1 && f[2] <= 3) || (f[2] >= 9 && f[2] <= 11)))
         return load_tga(f, img, width, height, comps, err);
-    return err = "unsupported image format (PNG, BMP, TGA, Radiance HDR and binary PGM are read)", false;
+    return err = "unsupported image format (PNG, JPEG, BMP, TGA, Radiance HDR and binary PGM are read)", false;
 }
 
 bool load_gray(const std::string &path, std::vector<float> &img, int &width, int &height, std::string &err) {

@@ -9,15 +9,23 @@
 //   * binary PGM (P5, 8-bit), converted like 8-bit PNG gray;
 //   * BMP (1/4/8-bit palettes, 16/32-bit bit fields of up to 8 bits, 24/32-bit; bottom-up or top-down; no
 //     RLE) and TGA (color-mapped, truecolor 15/16/24/32-bit, gray 8/16-bit; raw or run-length), as
-//     stb reads them, then converted like 8-bit PNG.
+//     stb reads them, then converted like 8-bit PNG;
+//   * baseline JPEG (1 or 3 components, any sampling factors, restart intervals; jpeg.cpp): the Y plane
+//     of a YCbCr image, or the luma of an RGB-coded one, converted like 8-bit PNG.
 // Writing produces a Radiance .hdr (RGBE, run-length scanlines for widths 8..32767), gray stored as
 // R = G = B, as stbi_write_hdr does for one channel (src/v4_1_lpa_ici_2D_sparse_shared.cu:388, :522).
 #pragma once
 
+#include <cstdint>
 #include <string>
 #include <vector>
 
 namespace lpaici_cli {
+
+// Baseline JPEG to 8-bit samples with comps 1 (gray) or 3 (RGB) channels as stb_image computes them
+// (jpeg.cpp); false with err on failure (progressive files included).
+bool decode_jpeg(const std::vector<uint8_t> &file, int comps, std::vector<uint8_t> &px, int &width, int &height,
+                 std::string &err);
 
 // Returns false and sets err on failure.
 bool load_gray(const std::string &path, std::vector<float> &img, int &width, int &height, std::string &err);
