@@ -490,6 +490,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         plan.close()
         extra["batched_one_image"] = {"size": size, "value": px / (np.mean(b_ms) * 1e-3) / 1e6,
                                       "plain": value, "unit": UNIT, "graph": True, "bit_equal_to_plain": bool(same)}
+        extra["ffma"] = run_ffma(torch, lpaici, ks, x, out, clean, taps, peak, args, flush)
         ref_gpu = reference_gpu_v4_1(clean, noisy_h, out.cpu().numpy(), min(args.steps, 3))
         if "value" in ref_gpu:
             ref_gpu["ours_e2e_over_reference"] = (px / e2e_step / 1e6) / ref_gpu["value"]
@@ -664,6 +665,32 @@ def run_extras(torch, lpaici, ks, args, flush) -> dict:
     }
 
 
+def run_ffma(torch, lpaici, ks, x, exact_out, clean, taps, peak, args, flush) -> dict:
+    """The contracted mode (lpaici_forward_ffma: one fused multiply-add per tap) on the benchmark image:
+    its speed, its FP32 FMA fraction (same algorithmic taps), and its agreement with the exact forward
+    against the accuracy criteria of the goal (scale maps >= 99.99 %, max abs error <= 1e-4, PSNR within
+    0.01 dB)."""
+    H, W = x.shape
+    fo = torch.empty_like(x)
+    ms = time_launches(torch, lambda: lpaici.forward(ks, x, SIGMA, GAMMA, out=fo, ffma=True), args.steps, 1, flush)
+    _, emap = lpaici.forward(ks, x, SIGMA, GAMMA, out=exact_out, scale_map=True)
+    _, fmap = lpaici.forward(ks, x, SIGMA, GAMMA, out=fo, scale_map=True, ffma=True)
+    torch.cuda.synchronize()
+    agree = (emap == fmap)
+    px_agree = agree.all(dim=0)
+    diff = (fo.double() - exact_out.double()).abs()
+    a, b = fo.cpu().numpy(), exact_out.cpu().numpy()
+    t = float(np.mean(ms)) * 1e-3
+    return {"value": W * H / t / 1e6, "unit": UNIT, "ms": t * 1e3,
+            "roofline_frac": 2.0 * taps / t / peak["ffma_ops_per_s"],
+            "vs_exact": {"map_agreement": float(agree.double().mean()),
+                         "pixels_with_a_flipped_scale": int((~px_agree).sum()),
+                         "max_abs_err": float(diff.max()),
+                         "max_abs_err_agreeing_pixels": float(diff[px_agree].max()),
+                         "pixels_over_1e-4": int((diff > 1e-4).sum()),
+                         "psnr_delta_db": float(lpaici.psnr(clean, a) - lpaici.psnr(clean, b))}}
+
+
 def adjoint_identity(torch, x, g, out, grad) -> float:
     """With the selection frozen the forward is linear in its input, out = J x, so
     sum(g * out) = sum(g * J x) = sum(J^T g * x) = sum(grad * x): the relative gap of the two sums
@@ -707,17 +734,31 @@ def run_profile(args) -> None:
     import lpaici
 
     tmp = tempfile.mkdtemp()
-    ks = lpaici.KernelSet.load(kernel_path(SYM, tmp))
+    gauss = args.kernels == "gauss_m2"
+    ks = lpaici.KernelSet.load(kernel_path(GAUSS_M2 if gauss else SYM, tmp))
     shutil.rmtree(tmp, ignore_errors=True)
+    sigma = float(np.float32(25.0) / np.float32(255.0)) if gauss else SIGMA
+    gamma = 1.5 if gauss else GAMMA
     if args.tile_config >= 0:
         ks.set_tile_config(args.tile_config)
-    _, noisy_h = bench_image(args.size, SEED, SIGMA)
-    x = torch.from_numpy(noisy_h).cuda()
-    out = torch.empty_like(x)
-    g = torch.randn(args.size, args.size, generator=torch.Generator().manual_seed(0)).cuda()
-    ops = {"forward": lambda: lpaici.forward(ks, x, SIGMA, GAMMA, out=out),
-           "adjoint": lambda: lpaici.backward(ks, x, g, SIGMA, GAMMA, grad_in=out)}
-    op = ops[args.profile]
+    if args.profile == "batched":  # the 64-image plan of the batched benchmark, one launch per step
+        from lpaici.synth import mixed_batch
+
+        spec = mixed_batch(64, SEED)
+        xs = [torch.from_numpy(lpaici.add_noise(lpaici.synth_image(w, h, i_s), s, n_s)).cuda()
+              for w, h, s, _, i_s, n_s in spec]
+        outs = [torch.empty_like(t) for t in xs]
+        plan = lpaici.Batch(ks, xs, outs, [v[2] for v in spec], [v[3] for v in spec], use_graph=True)
+        op = plan.run
+    else:
+        _, noisy_h = bench_image(args.size, SEED, sigma)
+        x = torch.from_numpy(noisy_h).cuda()
+        out = torch.empty_like(x)
+        g = torch.randn(args.size, args.size, generator=torch.Generator().manual_seed(0)).cuda()
+        ops = {"forward": lambda: lpaici.forward(ks, x, sigma, gamma, out=out),
+               "ffma": lambda: lpaici.forward(ks, x, sigma, gamma, out=out, ffma=True),
+               "adjoint": lambda: lpaici.backward(ks, x, g, sigma, gamma, grad_in=out)}
+        op = ops[args.profile]
     for _ in range(args.warmup):
         op()
     torch.cuda.synchronize()
@@ -740,8 +781,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--size", type=int, default=SIZE, help="image side (profiling runs use a smaller case)")
     ap.add_argument("--tile-config", type=int, default=-1, help="fixed tile configuration instead of autotuning")
-    ap.add_argument("--profile", choices=["forward", "adjoint"], default=None,
-                    help="run only this operation on one --size image (for profiler captures; no bench line)")
+    ap.add_argument("--profile", choices=["forward", "ffma", "adjoint", "batched"], default=None,
+                    help="run only this operation on one --size image, or the 64-image batched plan (for "
+                         "profiler captures; no bench line)")
+    ap.add_argument("--kernels", choices=["sym", "gauss_m2"], default="sym",
+                    help="kernel set of a --profile run: the 16x7 symmetric set (sigma 20/255, gamma 2) or the "
+                         "gaussian m=(2,0) set (sigma 25/255, gamma 1.5)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -57,6 +57,8 @@ typedef struct {
     int n_taps;       /* weights kept by the run-length packer (nonzeros + interior zeros of runs) */
     int n_runs;       /* row runs over all kernels */
     int radius;       /* largest |tap offset| from the kernel centre, rows or columns */
+    int blob_bytes;   /* device copy of the forward's packed kernels (one per device, made on first use) */
+    int adjoint_blob_bytes; /* device copy of the adjoint's mirrored kernels (one per device) */
 } lpaici_kernelset_info_t;
 
 /* Reads a kernel file: "D S", then D*S blocks "rows cols w[rows*cols]" in row-major order, and
@@ -82,6 +84,30 @@ int lpaici_kernelset_create(const float *weights, const int *offsets, const int 
  * command line's -k accepts it: the loader skips the text parse and rebuilds the same kernel set
  * (dense values outside the runs come back as +0).  No counterpart in the reference. */
 int lpaici_kernelset_save(const lpaici_kernelset *ks, const char *path);
+
+/* Kernel generation.  The reference ships its kernel files precomputed by a MATLAB LASIP script that is
+ * not in its tree (readme.md "Kernel files"); this generates directional LPA kernels of the same form
+ * from their definition: D directions (direction d points at angle 2*pi*d/D, counter-clockwise from +x,
+ * image rows down), one kernel per scale h = scales[s] on a (2h-1) x (2h-1) grid centred on the pixel.
+ * With u the distance along the direction and v across it, the support is
+ *   LPAICI_SHAPE_SECTOR:   the origin and every pixel with u < h - 1/2 whose angle from the direction
+ *                          is at most pi/D (a wedge, the directions tiling the plane);
+ *   LPAICI_SHAPE_QUADRANT: 0 <= u <= h - 1 and -(h - 1) <= v <= 0 (an h x h square on one side);
+ * and the weights are the local polynomial approximation of order `order` in u (0 .. 4; lowered to the
+ * number of distinct u values less one) with a uniform window, evaluated at the pixel: the least-squares
+ * fit of sum_q b_q u^q to the support, whose weights sum to 1.  Order 0 sectors reproduce
+ * kernels/lpa_kernels_m_1_0_d_16_h12_1_2_4_8_16_24_32_symmetric.txt (the default set), order 0 and 1
+ * quadrants the d_4_square sets, once written as text and read back (lpaici_kernelset_write_text prints 6
+ * decimals, as those files do): bit for bit, up to the sign of weights that are zero in exact arithmetic.  The Gaussian-window sets are not
+ * of this form.  No counterpart in the reference's code. */
+#define LPAICI_SHAPE_SECTOR 0
+#define LPAICI_SHAPE_QUADRANT 1
+int lpaici_kernelset_generate(int num_dirs, int num_scales, const int *scales, int order, int shape,
+                              lpaici_kernelset **out);
+
+/* Writes the dense kernels in the reference's text format (readme.md:95-103): "D S", then per kernel
+ * "rows cols" and its weights row by row, each printed "%f " on one line. */
+int lpaici_kernelset_write_text(const lpaici_kernelset *ks, const char *path);
 
 int lpaici_kernelset_destroy(lpaici_kernelset *ks);
 
@@ -118,6 +144,17 @@ int lpaici_kernel_variances(const lpaici_kernelset *ks, float sigma, float *var)
 int lpaici_forward(const lpaici_kernelset *ks, const float *d_noisy, int noisy_pitch, float *d_denoised,
                    int out_pitch, int width, int height, float sigma, float gamma, uint8_t *d_scale_map,
                    lpaici_stream_t stream);
+
+/* lpaici_forward with every tap computed as one fused multiply-add (product and sum rounded once)
+ * instead of a separately rounded product and sum: faster, and NOT bit-exact with the reference,
+ * whose CPU build rounds both.  The selected scales can differ where an interval test is a tie at
+ * FP32 rounding, which moves that pixel's output by up to about 1e-3 (measured figures in DESIGN.md);
+ * everywhere else the output differs from lpaici_forward's by a few ULP.  Same arguments and errors as
+ * lpaici_forward.  No counterpart in the reference (whose GPU builds let the compiler contract some of
+ * its multiply-adds). */
+int lpaici_forward_ffma(const lpaici_kernelset *ks, const float *d_noisy, int noisy_pitch, float *d_denoised,
+                        int out_pitch, int width, int height, float sigma, float gamma, uint8_t *d_scale_map,
+                        lpaici_stream_t stream);
 
 /* As lpaici_forward, with the per-kernel variances given by the caller (host array, D*S floats)
  * instead of sigma, as the reference's engine receives them (host_kernel_variances,

@@ -2,18 +2,24 @@
 //
 // For L = sum_p g[p] * out[p] and the selected scale s*(d,p) of every direction and pixel frozen,
 // out is linear in the input x:  out(p) = sum_d alpha_d(p) * sum_t h_{d,s*}(t) x(p + t - c), with
-// alpha_d(p) = (1/v_{d,s*}) / den(p), den(p) = sum_d' 1/v_{d',s*}.  Hence, with u(p) = g(p) / den(p),
-//     dL/dx(q) = sum_d sum_s (1/v_{d,s}) sum_t h_{d,s}(t) [s*(d, q - t + c) = s] u(q - t + c)   (zero padding)
-// i.e. for every direction and scale, a correlation of the masked field u [s*(d,.) = s] with the kernel
-// mirrored through its centre and scaled by 1/v.  Two launches:
+// alpha_d(p) = (1/v_{d,s*}) / den(p), den(p) = sum_d' 1/v_{d',s*}.  With the adjoint field of direction d
+//     c_d(p) = g(p) / den(p) / v_{d, s*(d,p)},
+//     dL/dx(q) = sum_d sum_s sum_t h'_{d,s}(t) [s*(d, q + t) = s] c_d(q + t)       (zero padding)
+// where h' is h mirrored through its centre: for every direction and scale, a correlation of the field
+// masked to the pixels that selected that scale.  Two launches:
 //   A. selection: the forward's exact tile sweep recomputes s*(d,p) (one byte per direction and
 //      pixel) and 1/den(p) into a transient workspace -- the forward stores nothing for the adjoint;
-//   B. gather: one CTA per output tile builds u on the tile plus its R-pixel halo in shared memory
-//      once, and s*(d,.) there per direction; per scale present it masks u -- only over the rectangle
-//      that scale's mirrored kernel reaches from the tile -- and correlates it with the mirrored
-//      kernel's row runs (register sliding window, 9 outputs per thread, FFMA -- the adjoint is checked
-//      against FP64 finite differences, not bit patterns).  Every output is written once: no atomics,
-//      deterministic.
+//   B. gather: one CTA per output tile.  It builds u = g / den on the tile plus its R-pixel halo in
+//      shared memory once; per direction it loads s*(d,.) there and forms the field c_d = u / v_{d,s*}.
+//      The kernels are telescoped, D_s = h'_s - h'_{s-1} (D_0 = h'_0, built by kernelset.cpp), which
+//      turns the sum over scales into
+//          sum_s D_s (*) (c_d [s* >= s]):
+//      the field is zeroed in place where s* < s, scale after scale (only where the next kernel
+//      reaches), and never rebuilt.  The runs are the forward's run loop (register sliding window over
+//      Q columns, exact-length tails) with packed FMAs over two output rows -- the adjoint is checked
+//      against FP64 finite differences, not bit patterns.  Groups of warps take every G-th run of each
+//      kernel over the same outputs and add their sums in group order at the end.  Every output is
+//      written once: no atomics, deterministic.
 // No counterpart in the reference.
 #include <algorithm>
 #include <cmath>
@@ -28,23 +34,51 @@ namespace lpaici {
 
 namespace {
 
-constexpr int kGatherP = 9;  // output columns per thread (odd: conflict-free scalar shared loads)
+// Gather tile geometry.  A lane owns output rows ty and ty + 8 at Q = 8 consecutive columns and keeps
+// them as the two halves of packed FMAs; a warp covers 16 rows x 32 columns: lane l has row index
+// a = l & 7 and column group b = l >> 3.  The fields are plain row-major float arrays whose pitch p is
+// 1 mod 8, so the 32 lanes' scalar loads of one row hit 32 different banks (a*p gives the residues
+// mod 8, 8b the multiples of 8).  kGatherWX warps across and WY down make one group; kGatherG groups
+// cover the same outputs, each with every G-th run of a kernel.  Eight columns per lane spread each
+// run's loop, window preload and tail over 16 outputs.
+constexpr int kGatherQ = 8;
+constexpr int kGatherPair = 8;  // rows between a lane's two output rows
 constexpr int kGatherWX = 2;
-constexpr int kGatherTW = kGatherWX * 4 * kGatherP;  // 72 output columns; 8 * WY rows (WY = 8: 64)
-// A warp covers 16 output rows x 36 columns: lane l owns rows y and y + 8 (y = l / 4 within the warp's
-// 8-row band) at 9 columns, and computes the two rows in the halves of packed f32x2 FMAs.  Four groups
-// of warps cover the same outputs, each with every fourth run of a kernel; their partial sums are added
-// at the end.
-constexpr int kGatherGroups = 4;
+constexpr int kGatherG = 4;
+constexpr int kGatherWarpCols = 32 / kGatherPair * kGatherQ;  // columns one warp covers
 template <int WY>
 struct GatherShape {
-    static_assert(WY % 2 == 0, "a warp covers 16 rows");
-    static constexpr int kTH = 8 * WY;
-    static constexpr int kGroupThreads = 32 * kGatherWX * (WY / 2);
-    static constexpr int kThreads = kGatherGroups * kGroupThreads;
+    static constexpr int kTW = kGatherWarpCols * kGatherWX;
+    static constexpr int kTH = 2 * kGatherPair * WY;
+    static constexpr int kGroupThreads = 32 * kGatherWX * WY;
+    static constexpr int kThreads = kGatherG * kGroupThreads;
 };
-// Tile heights the host can choose (the tallest whose fields and mirrored kernels fit in shared memory).
-constexpr int kGatherWYs[] = {8, 6, 4, 2};
+// Tile heights the host can choose (the tallest whose fields and kernels fit in shared memory).
+constexpr int kGatherWYs[] = {4, 3, 2, 1};
+
+// Field geometry: rows th + 2R, pitch 1 mod 8 and >= tw + 2R + Q (a margin no load reaches).
+struct GatherGeom {
+    int rows, pitch;
+    __host__ __device__ static GatherGeom make(int tw, int th, int R) {
+        GatherGeom g;
+        g.rows = th + 2 * R;
+        g.pitch = ((tw + 2 * R + kGatherQ + 6) & ~7) + 1;
+        return g;
+    }
+    __host__ __device__ size_t cells() const { return static_cast<size_t>(rows) * pitch; }
+};
+
+// Window of a run over a field: column i is the pair {a[i], b[i]} of the lane's two rows (b = a +
+// kGatherPair rows).  Both pointers advance with the taps, so every load has a constant offset.
+struct PairWin {
+    const float *a, *b;
+    __device__ __forceinline__ float2 operator[](int i) const { return make_float2(a[i], b[i]); }
+    __device__ __forceinline__ PairWin &operator+=(int n) {
+        a += n;
+        b += n;
+        return *this;
+    }
+};
 
 // One image of the gather: pass A's outputs and the caller's buffers.
 struct GatherImage {
@@ -62,95 +96,37 @@ struct GatherArgs {
     const GatherImage *images;   // batched: per-image descriptors in device memory
     const int2 *items;           // batched: (image, tile) of every CTA
     int D, S, R;
-    const int *blob;       // mirrored kernels (lpaici_kernelset::adj_blob)
+    const int *blob;       // mirrored kernels (lpaici_kernelset::adj_blob, BlobLayout)
     int blob_words, run_word, weight_word;
-    int pitch, rows;       // shared-memory field geometry (floats)
+    int pitch, rows;       // field geometry (GatherGeom of the tile)
     int th;                // output rows per tile
     float rvar[kMaxKernels];  // 1 / v_k of the one image
-    // per kernel: the field rectangle its gathers read, rows [x, y), 4-column groups [z, w)
+    // per kernel: the field cells its correlation reads, rows [x, y), columns [z, w); per direction: the
+    // union over its scales (the cells its field needs)
     int4 rect[kMaxKernels];
+    int4 drect[kMaxKernels];
 };
 
-// Smallest pitch >= need with (pitch / 4) odd: scalar loads of 8 rows x 4 column groups of 9 hit 32
-// different banks.
-__host__ __device__ inline int field_pitch(int need) {
-    int p = (need + 3) & ~3;
-    if (((p >> 2) & 1) == 0) p += 4;
-    return p;
-}
-
-// Copies the mirrored blob like stage_words and folds each run's (dy, dx0) into its offset
-// dy * pitch + dx0 in the field, on the way: the run becomes (offset, 0, len, weight index).  Runs
-// occupy words [run_word, weight_word).
-__device__ __forceinline__ void stage_adj_blob(int *dst, const int *__restrict__ src, int words, int run_word,
-                                               int weight_word, int pitch) {
-    const int4 *s = reinterpret_cast<const int4 *>(src);
-    int4 *d = reinterpret_cast<int4 *>(dst);
-    const int r0 = run_word >> 2, r1 = weight_word >> 2;
-    for (int i = threadIdx.x; i < (words >> 2); i += blockDim.x) {
-        int4 v = __ldg(s + i);
-        if (i >= r0 && i < r1) v = make_int4(v.x * pitch + v.y, 0, v.z, v.w);
-        d[i] = v;
-    }
-}
-
-// d = a * b + c in each half, rounded on its own (the two halves of fmaf).
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
-    float2 d;
-    asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\t"
-        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
-        "fma.rn.f32x2 rd, ra, rb, rc;\n\t"
-        "mov.b64 {%0, %1}, rd;\n\t}"
-        : "=f"(d.x), "=f"(d.y)
-        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
-    return d;
-}
-
-// acc[i] += sum_{j < len} w[j] * {src[i + j], src[i + j + pair]} for the thread's P output columns in
-// its two rows (sliding window).  Reads src[0, len + P - 1) and the same span at src + pair.  The
-// pointers advance with the taps, so every load has a constant offset.
-template <int P>
-__device__ __forceinline__ void gather_run(float2 (&acc)[P], const float *__restrict__ src, int pair,
-                                           const float *__restrict__ w, int len) {
-    const float *__restrict__ src2 = src + pair;
-    float2 win[P];
-#pragma unroll
-    for (int i = 0; i < P - 1; i++) win[i] = make_float2(src[i], src2[i]);
-    for (; len >= P; len -= P, src += P, src2 += P, w += P) {
-#pragma unroll
-        for (int j = 0; j < P; j++) {
-            win[(j + P - 1) % P] = make_float2(src[j + P - 1], src2[j + P - 1]);
-            const float wt = w[j];
-            const float2 w2 = make_float2(wt, wt);
-#pragma unroll
-            for (int i = 0; i < P; i++) acc[i] = fma2(w2, win[(j + i) % P], acc[i]);
-        }
-    }
-#pragma unroll
-    for (int j = 0; j < P - 1; j++) {
-        if (j >= len) break;
-        win[(j + P - 1) % P] = make_float2(src[j + P - 1], src2[j + P - 1]);
-        const float wt = w[j];
-        const float2 w2 = make_float2(wt, wt);
-#pragma unroll
-        for (int i = 0; i < P; i++) acc[i] = fma2(w2, win[(j + i) % P], acc[i]);
-    }
+// Shared memory: blob (runs as field offsets) | 1/v table | u | field | selected scales.
+__host__ __device__ inline int rv_words(int nk) { return (nk + 3) & ~3; }
+// The scale map carries 4 bytes past its last cell, set to 0xff: the masking reads it in whole words.
+__host__ __device__ inline size_t gather_smem(int blob_words, int nk, const GatherGeom &g) {
+    return sizeof(int) * (blob_words + rv_words(nk)) + 2 * sizeof(float) * g.cells() + ((g.cells() + 4 + 15) & ~size_t(15));
 }
 
 template <int WY>
 __global__ void __launch_bounds__(GatherShape<WY>::kThreads, 1)
     lpaici_adjoint_gather_kernel(const __grid_constant__ GatherArgs a) {
-    constexpr int P = kGatherP;
-    constexpr int kGatherTH = GatherShape<WY>::kTH;
-    constexpr int kGroupThreads = GatherShape<WY>::kGroupThreads;
-    constexpr int kGatherThreads = GatherShape<WY>::kThreads;
+    using Shape = GatherShape<WY>;
+    constexpr int Q = kGatherQ, G = kGatherG;
     extern __shared__ __align__(16) int smem[];
-    __shared__ unsigned s_present;
-    const int fsize = a.rows * a.pitch;  // a multiple of 4
+    const int nk = a.D * a.S;
+    const int cells = a.rows * a.pitch;
     int *s_blob = smem;
-    float *s_u = reinterpret_cast<float *>(smem + a.blob_words);  // u = g / den on the halo'd tile
-    float *s_f = s_u + fsize;                                     // the masked field of one kernel
-    uint8_t *s_s = reinterpret_cast<uint8_t *>(s_f + fsize);      // s*(d, .) on the halo'd tile
+    float *s_rv = reinterpret_cast<float *>(smem + a.blob_words);
+    float *s_u = s_rv + rv_words(nk);  // u = g / den on the halo'd tile, once per tile
+    float *s_f = s_u + cells;          // the field of the current direction
+    uint8_t *s_s = reinterpret_cast<uint8_t *>(s_f + cells);  // s*(d, .) on the halo'd tile
     GatherImage im;
     int tile = blockIdx.x;
     if (a.images) {
@@ -161,125 +137,120 @@ __global__ void __launch_bounds__(GatherShape<WY>::kThreads, 1)
         im = a.single;
     }
     const float *rvar_k = a.images ? im.rvar : a.rvar;
-    const int x0 = (tile % im.tiles_x) * kGatherTW, y0 = (tile / im.tiles_x) * kGatherTH;
+    const int x0 = (tile % im.tiles_x) * Shape::kTW, y0 = (tile / im.tiles_x) * Shape::kTH;
     const int gx0 = x0 - a.R, gy0 = y0 - a.R;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = kGatherThreads >> 5;
-    const int group = threadIdx.x / kGroupThreads, gtid = threadIdx.x % kGroupThreads, gwarp = gtid >> 5;
-    const int ty = (gwarp / kGatherWX) * 16 + (lane >> 2);  // and ty + 8
-    const int tx = (gwarp % kGatherWX) * 4 * P + (lane & 3) * P;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = Shape::kThreads >> 5;
+    // the group is the same in every lane of a warp: reduced, the compiler knows it warp-uniform, so the
+    // run loops and the tails' dispatch branch without reconvergence bookkeeping
+    const int group = __reduce_max_sync(0xffffffffu, static_cast<unsigned>(threadIdx.x / Shape::kGroupThreads));
+    const int gtid = threadIdx.x % Shape::kGroupThreads;
+    const int gwarp = gtid >> 5;
+    const int ty = (gwarp / kGatherWX) * 2 * kGatherPair + (lane & (kGatherPair - 1));  // and ty + kGatherPair
+    const int tx = (gwarp % kGatherWX) * kGatherWarpCols + (lane / kGatherPair) * Q;
+    const int lane_off = (ty + a.R) * a.pitch + tx + a.R;
+    const int pair_rows = kGatherPair * a.pitch;
     const int4 *s_runs = reinterpret_cast<const int4 *>(s_blob + a.run_word);
-    float *s_w = reinterpret_cast<float *>(s_blob + a.weight_word);
-    const float *lane_f = s_f + (ty + a.R) * a.pitch + tx + a.R;
-    const int groups = a.pitch >> 2;
-    const int nk = a.D * a.S;
+    const float4 *s_wq = reinterpret_cast<const float4 *>(s_blob + a.weight_word);
 
-    stage_adj_blob(s_blob, a.blob, a.blob_words, a.run_word, a.weight_word, a.pitch);
+    stage_blob(s_blob, a.blob, a.blob_words, a.run_word, a.weight_word, a.pitch);
+    for (int k = threadIdx.x; k < nk; k += blockDim.x) s_rv[k] = rvar_k[k];
+    if (threadIdx.x < 4) s_s[cells + threadIdx.x] = 0xff;  // never below a scale: the masking leaves it
     for (int r = warp; r < a.rows; r += nwarps) {  // one warp per row, lanes along it
         const int gy = gy0 + r;
         const bool row_ok = gy >= 0 && gy < im.H;
-        for (int cc = lane; cc < a.pitch; cc += 32) {
-            const int gx = gx0 + cc;
+        for (int c = lane; c < a.pitch; c += 32) {
+            const int gx = gx0 + c;
             float u = 0.0f;
             if (row_ok && gx >= 0 && gx < im.W)
-                u = im.g[static_cast<size_t>(gy) * im.g_pitch + gx] * im.rden[static_cast<size_t>(gy) * im.W + gx];
-            s_u[r * a.pitch + cc] = u;
+                u = __ldg(im.g + static_cast<size_t>(gy) * im.g_pitch + gx) *
+                    __ldg(im.rden + static_cast<size_t>(gy) * im.W + gx);
+            s_u[r * a.pitch + c] = u;
         }
     }
-    __syncthreads();
-    // alpha's 1/v_k moves into kernel k's weights: sum_t (w_t / v_k) u(p_t); a kernel's weights are
-    // contiguous, one warp scales them
-    for (int k = warp; k < nk; k += nwarps) {
-        const int r0 = s_blob[k], r1 = s_blob[k + 1];
-        if (r0 == r1) continue;
-        const int w0 = s_runs[r0].w, w1 = s_runs[r1 - 1].w + s_runs[r1 - 1].z;
-        const float rv = rvar_k[k];
-        for (int i = w0 + lane; i < w1; i += 32) s_w[i] *= rv;
-    }
 
-    float2 acc[P];
+    float2 acc[Q];
 #pragma unroll
-    for (int i = 0; i < P; i++) acc[i] = make_float2(0.0f, 0.0f);
-    const int pair = 8 * a.pitch;
+    for (int i = 0; i < Q; i++) acc[i] = make_float2(0.0f, 0.0f);
+    const FmaTap tap;
 
     for (int d = 0; d < a.D; d++) {
-        __syncthreads();  // weights scaled; the previous direction's gathers are done with s_s / s_f
-        if (threadIdx.x == 0) s_present = 0u;
-        __syncthreads();
-        unsigned present = 0;
+        __syncthreads();  // u and the tables staged; the previous direction's correlations are done
+        // s*(d, .) and c_d = u / v_{d, s*} where the direction's kernels reach (u is 0 outside the
+        // image); the other cells keep stale values that no correlation of this direction reads
         const uint8_t *plane = im.smap + static_cast<size_t>(d) * im.H * im.W;
-        for (int r = warp; r < a.rows; r += nwarps) {
+        const float *rv_d = s_rv + d * a.S;
+        const int4 dr = a.drect[d];
+        for (int r = dr.x + warp; r < dr.y; r += nwarps) {
             const int gy = gy0 + r;
             const bool row_ok = gy >= 0 && gy < im.H;
-            for (int cc = lane; cc < a.pitch; cc += 32) {
-                const int gx = gx0 + cc;
-                uint8_t s = 0xff;
-                if (row_ok && gx >= 0 && gx < im.W) {
-                    s = plane[static_cast<size_t>(gy) * im.W + gx];
-                    present |= 1u << s;
-                }
-                s_s[r * a.pitch + cc] = s;
+            const uint8_t *prow = plane + static_cast<size_t>(row_ok ? gy : 0) * im.W;
+            for (int c = dr.z + lane; c < dr.w; c += 32) {
+                const int gx = gx0 + c;
+                const unsigned sc = row_ok && gx >= 0 && gx < im.W ? __ldg(prow + gx) : 0u;
+                const int i = r * a.pitch + c;
+                s_s[i] = static_cast<uint8_t>(sc);
+                s_f[i] = s_u[i] * rv_d[sc];
             }
         }
-        present = __reduce_or_sync(0xffffffffu, present);
-        if (lane == 0) atomicOr(&s_present, present);
         __syncthreads();
-        const unsigned mask = s_present;
+        // telescoped scales: zero the field where s* < s, as far as D_s reaches, then correlate
         for (int s = 0; s < a.S; s++) {
-            if (!(mask & (1u << s))) continue;  // block-uniform
             const int k = d * a.S + s;
-            const int4 rc = a.rect[k];
-            const float4 *u4 = reinterpret_cast<const float4 *>(s_u);
-            const uchar4 *s4 = reinterpret_cast<const uchar4 *>(s_s);
-            float4 *f4 = reinterpret_cast<float4 *>(s_f);
-            for (int r = rc.x + warp; r < rc.y; r += nwarps) {
-                for (int q = rc.z + lane; q < rc.w; q += 32) {
-                    const int i = r * groups + q;
-                    const float4 u = u4[i];
-                    const uchar4 m = s4[i];
-                    f4[i] = make_float4(m.x == s ? u.x : 0.0f, m.y == s ? u.y : 0.0f, m.z == s ? u.z : 0.0f,
-                                        m.w == s ? u.w : 0.0f);
+            if (s > 0) {
+                const int4 rc = a.rect[k];
+                const unsigned below = 0x01010101u * static_cast<unsigned>(s);
+                __syncthreads();  // every correlation of the previous scale is done with the field
+                // whole 4-cell words of the scale map (a word may reach past the rectangle: zeroing a cell
+                // with s* < s anywhere keeps the field c_d [s* >= s]); 4-byte aligned, as s_s is
+                for (int r = rc.x + warp; r < rc.y; r += nwarps) {
+                    const int w0 = (r * a.pitch + rc.z) >> 2, w1 = (r * a.pitch + rc.w + 3) >> 2;
+                    const unsigned *srow = reinterpret_cast<const unsigned *>(s_s);
+                    for (int wi = w0 + lane; wi < w1; wi += 32) {
+                        const unsigned lt = __vcmpltu4(srow[wi], below);  // 0xff per byte with s* < s
+                        if (lt) {
+                            float *f = s_f + 4 * wi;
+#pragma unroll
+                            for (int b = 0; b < 4; b++)
+                                if (lt & (0xffu << (8 * b))) f[b] = 0.0f;
+                        }
+                    }
                 }
+                __syncthreads();
             }
-            __syncthreads();
-            // the run descriptors are the same in every lane: reduced, they are known warp-uniform, so
-            // the loop and the tail's exits branch without reconvergence bookkeeping
-            const int r_end = __reduce_max_sync(0xffffffffu, s_blob[k + 1]);
-            for (int r = __reduce_max_sync(0xffffffffu, s_blob[k] + group); r < r_end; r += kGatherGroups) {
-                const int4 run = s_runs[r];
-                const int off = __reduce_max_sync(0xffffffffu, run.x);  // dy * pitch + dx0: stage_adj_blob
-                const int wo = __reduce_max_sync(0xffffffffu, run.w);
-                const int len = __reduce_max_sync(0xffffffffu, run.z);
-                gather_run<P>(acc, lane_f + off, pair, s_w + wo, len);
+            const int r_end = s_blob[k + 1];
+            for (int r = s_blob[k] + group; r < r_end; r += G) {
+                const int4 run = s_runs[r];  // (field offset, len, float4 weight index): see stage_blob
+                const int o = lane_off + run.x;
+                conv_run<Q>(acc, PairWin{s_f + o, s_f + o + pair_rows}, s_wq + run.z, run.y, tap);
             }
-            __syncthreads();  // before the next kernel's field overwrites s_f
         }
     }
-    // groups 1, 2, ... hand their partial sums to group 0 in turn through s_f (free after the last
+    // groups 1, 2, ... hand their partial sums to group 0 in turn through the field (free after the
     // barrier); group 0 adds them in group order
     float2 *s_h = reinterpret_cast<float2 *>(s_f);
-    for (int g = 1; g < kGatherGroups; g++) {
+    for (int g = 1; g < G; g++) {
+        __syncthreads();
         if (group == g) {
 #pragma unroll
-            for (int i = 0; i < P; i++) s_h[i * kGroupThreads + gtid] = acc[i];
+            for (int i = 0; i < Q; i++) s_h[i * Shape::kGroupThreads + gtid] = acc[i];
         }
         __syncthreads();
         if (group == 0) {
 #pragma unroll
-            for (int i = 0; i < P; i++) {
-                const float2 other = s_h[i * kGroupThreads + gtid];
+            for (int i = 0; i < Q; i++) {
+                const float2 other = s_h[i * Shape::kGroupThreads + gtid];
                 acc[i] = make_float2(acc[i].x + other.x, acc[i].y + other.y);
             }
         }
-        __syncthreads();
     }
     if (group == 0) {
 #pragma unroll
         for (int h = 0; h < 2; h++) {
-            const int oy = y0 + ty + 8 * h;
+            const int oy = y0 + ty + kGatherPair * h;
             if (oy >= im.H) break;
             float *o = im.grad + static_cast<size_t>(oy) * im.grad_pitch + x0 + tx;
 #pragma unroll
-            for (int i = 0; i < P; i++)
+            for (int i = 0; i < Q; i++)
                 if (x0 + tx + i < im.W) o[i] = h == 0 ? acc[i].x : acc[i].y;
         }
     }
@@ -289,44 +260,46 @@ __global__ void __launch_bounds__(GatherShape<WY>::kThreads, 1)
 
 namespace {
 
-// The launch-independent part of the gather's arguments: field geometry, mirrored kernels and the
-// per-kernel rectangles; smem receives the dynamic shared memory, checked against the device.
 template <int WY>
 const void *gather_fn() {
     return reinterpret_cast<const void *>(lpaici_adjoint_gather_kernel<WY>);
 }
 const void *gather_fn(int wy) {
     switch (wy) {
-        case 8: return gather_fn<8>();
-        case 6: return gather_fn<6>();
         case 4: return gather_fn<4>();
-        default: return gather_fn<2>();
+        case 3: return gather_fn<3>();
+        case 2: return gather_fn<2>();
+        default: return gather_fn<1>();
     }
 }
 
 int gather_launch(const GatherArgs &ga, int wy, unsigned grid, size_t smem, cudaStream_t stream) {
     switch (wy) {
-        case 8: lpaici_adjoint_gather_kernel<8><<<grid, GatherShape<8>::kThreads, smem, stream>>>(ga); break;
-        case 6: lpaici_adjoint_gather_kernel<6><<<grid, GatherShape<6>::kThreads, smem, stream>>>(ga); break;
         case 4: lpaici_adjoint_gather_kernel<4><<<grid, GatherShape<4>::kThreads, smem, stream>>>(ga); break;
-        default: lpaici_adjoint_gather_kernel<2><<<grid, GatherShape<2>::kThreads, smem, stream>>>(ga); break;
+        case 3: lpaici_adjoint_gather_kernel<3><<<grid, GatherShape<3>::kThreads, smem, stream>>>(ga); break;
+        case 2: lpaici_adjoint_gather_kernel<2><<<grid, GatherShape<2>::kThreads, smem, stream>>>(ga); break;
+        default: lpaici_adjoint_gather_kernel<1><<<grid, GatherShape<1>::kThreads, smem, stream>>>(ga); break;
     }
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? LPAICI_OK : cuda_error(e, "adjoint gather launch");
 }
 
-// Chooses the tile height (*wy: 8 * wy output rows) and fills the geometry.
+// Chooses the tile height (*wy: 16 * wy output rows), fills the geometry and the per-kernel rectangles of
+// the in-place masking; smem receives the dynamic shared memory, checked against the device.
 int gather_setup(const lpaici_kernelset *ks, const int *adj_blob, GatherArgs *ga, size_t *smem, int *wy) {
+    const BlobLayout &L = ks->adj_layout;
+    const int nk = ks->D * ks->S;
     ga->R = ks->radius;
-    ga->pitch = field_pitch(kGatherTW + 2 * ga->R + kGatherP);
-    ga->blob_words = static_cast<int>(ks->adj_blob.size());
+    ga->blob_words = L.total_words;
     int dev = 0, max_optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     *wy = 0;
+    GatherGeom geo{};
+    constexpr int kTW = GatherShape<1>::kTW;
     for (const int w : kGatherWYs) {
-        const size_t fsize = static_cast<size_t>(ga->pitch) * (8 * w + 2 * ga->R);
-        *smem = sizeof(int) * ga->blob_words + 2 * sizeof(float) * fsize + fsize;
+        geo = GatherGeom::make(kTW, GatherShape<1>::kTH * w, ga->R);
+        *smem = gather_smem(L.total_words, nk, geo);
         if (*smem <= static_cast<size_t>(max_optin)) {
             *wy = w;
             break;
@@ -335,20 +308,21 @@ int gather_setup(const lpaici_kernelset *ks, const int *adj_blob, GatherArgs *ga
     if (*wy == 0)
         return set_error(LPAICI_ERR_UNSUPPORTED, "adjoint tile needs %zu B of shared memory, device allows %d", *smem,
                          max_optin);
-    ga->th = 8 * *wy;
-    ga->rows = ga->th + 2 * ga->R;
+    ga->th = GatherShape<1>::kTH * *wy;
+    ga->pitch = geo.pitch;
+    ga->rows = geo.rows;
     ga->D = ks->D;
     ga->S = ks->S;
     ga->blob = adj_blob;
-    ga->run_word = ks->adj_run_word;
-    ga->weight_word = ks->adj_weight_word;
-    const int nk = ks->D * ks->S;
+    ga->run_word = L.run_word;
+    ga->weight_word = L.weight_word;
     for (int k = 0; k < nk; k++) {
-        // output rows [0, TH) read field rows ty + R + dy; output columns [0, TW) read field columns
-        // tx + R + dx0 + [0, len + P - 1) for the thread's first output tx (a multiple of P)
+        // a lane reads rows ty + R + dy and ty + 8 + R + dy (ty + 8 < th) and columns
+        // tx + R + dx0 + [0, len + Q - 1) (tx + Q <= tile width): rows [R + dy_min, R + th + dy_max),
+        // columns [R + dx_min, R + tile width + dx_max)
         int ylo = 0, yhi = -1, xlo = 0, xhi = -1;
         for (int r = ks->adj_blob[k]; r < ks->adj_blob[k + 1]; r++) {
-            const int *run = &ks->adj_blob[ks->adj_run_word + 4 * r];
+            const int *run = &ks->adj_blob[L.run_word + 4 * r];
             const int dy = run[0], c0 = run[1], c1 = run[1] + run[2] - 1;
             if (yhi < ylo) {
                 ylo = yhi = dy;
@@ -361,12 +335,24 @@ int gather_setup(const lpaici_kernelset *ks, const int *adj_blob, GatherArgs *ga
                 xhi = std::max(xhi, c1);
             }
         }
-        if (yhi < ylo) {
+        if (yhi < ylo)
             ga->rect[k] = make_int4(0, 0, 0, 0);  // no taps
-        } else {
-            const int col_end = std::min(ga->pitch, ga->R + kGatherTW + xhi + 1);
-            ga->rect[k] = make_int4(ga->R + ylo, ga->R + ga->th + yhi, (ga->R + xlo) >> 2, (col_end + 3) >> 2);
+        else
+            ga->rect[k] = make_int4(std::max(0, ga->R + ylo), std::min(geo.rows, ga->R + ga->th + yhi),
+                                    std::max(0, ga->R + xlo), std::min(geo.pitch, ga->R + kTW + xhi));
+    }
+    for (int d = 0; d < ks->D; d++) {
+        int4 u = make_int4(0, 0, 0, 0);
+        for (int s = 0; s < ks->S; s++) {
+            const int4 r = ga->rect[d * ks->S + s];
+            if (r.y <= r.x || r.w <= r.z) continue;
+            if (u.y <= u.x) {
+                u = r;
+            } else {
+                u = make_int4(std::min(u.x, r.x), std::max(u.y, r.y), std::min(u.z, r.z), std::max(u.w, r.w));
+            }
         }
+        ga->drect[d] = u;
     }
     cudaError_t e = cudaFuncSetAttribute(gather_fn(*wy), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(*smem));
@@ -374,7 +360,7 @@ int gather_setup(const lpaici_kernelset *ks, const int *adj_blob, GatherArgs *ga
 }
 
 long gather_tiles(int width, int height, int th, int *tiles_x) {
-    *tiles_x = (width + kGatherTW - 1) / kGatherTW;
+    *tiles_x = (width + GatherShape<1>::kTW - 1) / GatherShape<1>::kTW;
     return static_cast<long>(*tiles_x) * ((height + th - 1) / th);
 }
 

@@ -39,6 +39,11 @@ struct BatchArgs {
     const int *blob;
     int blob_words, run_word, weight_word;
     float neg_zero;  // -0.0f, read at run time (see prod2 in tile_core.cuh)
+    // every image of the plan has the same sigma and gamma (always so for one image): its var and thr
+    // travel here, as in the single-image launch, instead of being read per CTA from `tables`
+    int shared_tables;
+    float var[kMaxKernels];
+    float thr[kMaxKernels];
 };
 
 template <int WX, int WY, int Q>
@@ -52,29 +57,42 @@ __global__ void __launch_bounds__(32 * WX * WY, 1)
     float2 *s_tile = reinterpret_cast<float2 *>(smem + a.blob_words + table_words(nk));
     const TileGeom g = TileGeom::make(Shape::kTileW, Shape::kTileH, a.R, Q);
 
+    // the CTA's image arguments live in shared memory: in registers they would stay live across the
+    // whole sweep, beside the run loop's (the single-image kernel reads them from its parameters)
+    __shared__ __align__(16) unsigned char s_img_raw[sizeof(ImageArgs)];
+    __shared__ int2 s_xy;
+    ImageArgs &s_img = *reinterpret_cast<ImageArgs *>(s_img_raw);
     const int item = blockIdx.x;  // one CTA per queue item, dispatched in queue order
     if (item >= a.n_items) return;
+    if (threadIdx.x == 0) {
+        const int2 it = a.items[item];
+        const BatchImage bi = a.images[it.x];
+        const int tiles_x = (bi.W + Shape::kTileW - 1) / Shape::kTileW;
+        ImageArgs img{};
+        img.in = bi.in;
+        img.out = bi.out;
+        img.smap = bi.smap;
+        img.rden = bi.rden;
+        img.W = bi.W;
+        img.in_h = bi.H;
+        img.in_pitch = bi.in_pitch;
+        img.out_pitch = bi.out_pitch;
+        img.row_begin = 0;
+        img.rows_out = bi.H;
+        s_img = img;
+        s_xy = make_int2((it.y % tiles_x) * Shape::kTileW, (it.y / tiles_x) * Shape::kTileH);
+    }
     stage_blob(s_blob, a.blob, a.blob_words, a.run_word, a.weight_word, g.pitch2);
-    const int2 it = a.items[item];
-    const BatchImage bi = a.images[it.x];
-    const float *t = a.tables + bi.tab_offset;
-    stage_tables(s_tab, t, t + nk, nk);
-    const int tiles_x = (bi.W + Shape::kTileW - 1) / Shape::kTileW;
-    const int x0 = (it.y % tiles_x) * Shape::kTileW, y0 = (it.y / tiles_x) * Shape::kTileH;
-    ImageArgs img{};
-    img.in = bi.in;
-    img.out = bi.out;
-    img.smap = bi.smap;
-    img.rden = bi.rden;
-    img.W = bi.W;
-    img.in_h = bi.H;
-    img.in_pitch = bi.in_pitch;
-    img.out_pitch = bi.out_pitch;
-    img.row_begin = 0;
-    img.rows_out = bi.H;
-    load_tile(s_tile, img, x0, y0, g);
+    if (a.shared_tables) stage_tables(s_tab, a.var, a.thr, nk);
     __syncthreads();
-    sweep_tile<WX, Q>(img, x0, y0, a.D, a.S, g, s_blob, a.run_word, a.weight_word, s_tab, s_tile, a.neg_zero);
+    if (!a.shared_tables) {
+        const float *t = a.tables + a.images[a.items[item].x].tab_offset;
+        stage_tables(s_tab, t, t + nk, nk);
+    }
+    const int x0 = s_xy.x, y0 = s_xy.y;
+    load_tile(s_tile, s_img, x0, y0, g);
+    __syncthreads();
+    sweep_tile<WX, Q>(s_img, x0, y0, a.D, a.S, g, s_blob, a.run_word, a.weight_word, s_tab, s_tile, a.neg_zero);
 }
 
 namespace {
@@ -227,6 +245,13 @@ int batch_plan_create(const lpaici_kernelset *ks, const BatchSpec *specs, int n,
     b->args.run_word = tab.run_word;
     b->args.weight_word = tab.weight_word;
     b->args.neg_zero = -0.0f;
+    bool same = true;
+    for (int i = 1; i < n; i++) same = same && specs[i].sigma == specs[0].sigma && specs[i].gamma == specs[0].gamma;
+    b->args.shared_tables = same ? 1 : 0;
+    if (same) {
+        std::memcpy(b->args.var, tables.data(), sizeof(float) * nk);
+        std::memcpy(b->args.thr, tables.data() + nk, sizeof(float) * nk);
+    }
 
     int max_optin = 0, per_sm = 0;
     cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device);

@@ -103,7 +103,7 @@ static int check_params(float sigma_or_one, float gamma) {
 static int forward_common(const lpaici_kernelset *ks, const float *d_in, int in_pitch, int width, int in_height,
                           int row_begin, int row_count, float *d_out, int out_pitch, const float *host_var,
                           float sigma, float gamma, uint8_t *d_smap, cudaStream_t stream, int step = 1,
-                          int config = -1) {
+                          int config = -1, bool fused = false) {
     if (!ks || !d_in || !d_out) return set_error(LPAICI_ERR_INVALID_ARG, "forward: null kernel set or image pointer");
     if (width <= 0 || in_height <= 0 || row_count <= 0)
         return set_error(LPAICI_ERR_INVALID_ARG, "forward: non-positive size %d x %d", width, row_count);
@@ -136,7 +136,7 @@ static int forward_common(const lpaici_kernelset *ks, const float *d_in, int in_
     KernelTables tab;
     fill_tables(ks, host_var, sigma, gamma, &tab);
     tab.blob = blob;
-    return launch_forward(ks, img, tab, config >= 0 ? config : config_for(ks, width, row_count), stream);
+    return launch_forward(ks, img, tab, config >= 0 ? config : config_for(ks, width, row_count), stream, fused);
 }
 
 // Every channel of an interleaved image (pixel (x, y), channel c at row y, float x * channels + c) as
@@ -164,6 +164,13 @@ int lpaici_forward(const lpaici_kernelset *ks, const float *d_noisy, int noisy_p
                    lpaici_stream_t stream) {
     return forward_common(ks, d_noisy, noisy_pitch, width, height, 0, height, d_denoised, out_pitch, nullptr, sigma,
                           gamma, d_scale_map, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int lpaici_forward_ffma(const lpaici_kernelset *ks, const float *d_noisy, int noisy_pitch, float *d_denoised,
+                        int out_pitch, int width, int height, float sigma, float gamma, uint8_t *d_scale_map,
+                        lpaici_stream_t stream) {
+    return forward_common(ks, d_noisy, noisy_pitch, width, height, 0, height, d_denoised, out_pitch, nullptr, sigma,
+                          gamma, d_scale_map, reinterpret_cast<cudaStream_t>(stream), 1, -1, true);
 }
 
 int lpaici_forward_var(const lpaici_kernelset *ks, const float *d_noisy, int noisy_pitch, float *d_denoised,

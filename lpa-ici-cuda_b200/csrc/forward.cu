@@ -11,7 +11,9 @@
 
 namespace lpaici {
 
-template <int WX, int WY, int Q>
+// Fused = false: every tap's product and sum rounded on their own (bit-exact with the reference);
+// true: each tap one fused multiply-add (lpaici_forward_ffma).
+template <int WX, int WY, int Q, bool Fused>
 __global__ void __launch_bounds__(32 * WX * WY, 1)
     lpaici_forward_kernel(const __grid_constant__ ImageArgs img, const __grid_constant__ KernelTables tab) {
     using Shape = TileShape<WX, WY, Q>;
@@ -27,19 +29,19 @@ __global__ void __launch_bounds__(32 * WX * WY, 1)
     stage_tables(s_tab, tab.var, tab.thr, nk);
     load_tile(s_tile, img, x0, y0, g);
     __syncthreads();
-    sweep_tile<WX, Q>(img, x0, y0, tab.D, tab.S, g, s_blob, tab.run_word, tab.weight_word, s_tab, s_tile,
-                   tab.neg_zero);
+    sweep_tile<WX, Q, Fused>(img, x0, y0, tab.D, tab.S, g, s_blob, tab.run_word, tab.weight_word, s_tab, s_tile,
+                             tab.neg_zero);
 }
 
 namespace {
 
-template <int WX, int WY, int Q>
+template <int WX, int WY, int Q, bool Fused>
 int launch_cfg(const ImageArgs &img, const KernelTables &tab, cudaStream_t stream) {
     using Shape = TileShape<WX, WY, Q>;
     const TileGeom g = TileGeom::make(Shape::kTileW, Shape::kTileH, tab.R, Q);
     const int nk = tab.D * tab.S;
     const size_t smem = sizeof(int) * (tab.blob_words + table_words(nk)) + g.tile_bytes();
-    auto kern = lpaici_forward_kernel<WX, WY, Q>;
+    auto kern = lpaici_forward_kernel<WX, WY, Q, Fused>;
     int dev = 0, max_optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
@@ -59,11 +61,11 @@ int launch_cfg(const ImageArgs &img, const KernelTables &tab, cudaStream_t strea
 }  // namespace
 
 #define LPAICI_FWD_CASE(idx, WX, WY, Q) \
-    case idx: return launch_cfg<WX, WY, Q>(img, tab, stream);
+    case idx: return fused ? launch_cfg<WX, WY, Q, true>(img, tab, stream) : launch_cfg<WX, WY, Q, false>(img, tab, stream);
 
 template <int WX, int WY, int Q>
 int blocks_per_sm(size_t smem) {
-    auto kern = lpaici_forward_kernel<WX, WY, Q>;
+    auto kern = lpaici_forward_kernel<WX, WY, Q, false>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) != cudaSuccess) {
         cudaGetLastError();
         return 0;
@@ -113,7 +115,7 @@ size_t config_smem(int config, int blob_words, int nk, int R) {
 }
 
 int launch_forward(const lpaici_kernelset *ks, const ImageArgs &img, const KernelTables &tab, int config,
-                   cudaStream_t stream) {
+                   cudaStream_t stream, bool fused) {
     (void)ks;
     if (tab.S > kMaxScales)
         return set_error(LPAICI_ERR_UNSUPPORTED, "%d scales per direction; the kernels support at most %d", tab.S,

@@ -82,9 +82,10 @@ struct lpaici_kernelset {
     int radius = 0;
     lpaici::BlobLayout layout;
     std::vector<int32_t> blob;  // host copy of the device blob
-    // the adjoint's flipped kernels (taps (-dy, -dx), weights reversed): [begin (nk+1)] [Run records
-    // {dy, dx0, len, weight index}] [float weights, 16 spare zeros]
-    int adj_run_word = 0, adj_weight_word = 0;
+    // the adjoint gather's kernels, mirrored through their centre (taps (-dy, -dx)), in the forward
+    // blob's layout (adj_layout): scale 0 as it is, every later scale as the difference from the scale
+    // before it (kernelset.cpp, build_adjoint_blob)
+    lpaici::BlobLayout adj_layout;
     std::vector<int32_t> adj_blob;
     // device copies, one per CUDA device, created on first use
     mutable std::mutex mu;
@@ -108,8 +109,10 @@ int device_adj_blob(const lpaici_kernelset *ks, const int **out);
 void fill_tables(const lpaici_kernelset *ks, const float *var_or_null, float sigma, float gamma, KernelTables *t);
 
 // Forward / backward launchers (forward.cu, backward.cu).
+// fused: each tap one fused multiply-add instead of a rounded product and a rounded sum (faster, not
+// bit-exact with the reference: lpaici_forward_ffma).
 int launch_forward(const lpaici_kernelset *ks, const ImageArgs &img, const KernelTables &tab, int config,
-                   cudaStream_t stream);
+                   cudaStream_t stream, bool fused = false);
 // Bytes of shared memory tile configuration `config` needs for a kernel set.
 size_t config_smem(int config, int blob_words, int nk, int R);
 // The autotuned configuration of ks on the current device, else the first one that fits.

@@ -2,6 +2,7 @@
 //
 // Host code; built with -ffp-contract=off so every float multiply and add rounds separately, as in
 // the reference's x86-64 build (no FMA without -march).
+#include <algorithm>
 #include <cerrno>
 #include <cmath>
 #include <cstdarg>
@@ -31,6 +32,87 @@ int set_error(int code, const char *fmt, ...) {
 int cuda_error(cudaError_t e, const char *what) {
     return set_error(e == cudaErrorMemoryAllocation ? LPAICI_ERR_NO_MEMORY : LPAICI_ERR_CUDA, "%s: %s (%s)", what,
                      cudaGetErrorString(e), cudaGetErrorName(e));
+}
+
+// ---------------------------------------------------------------------------------------------
+// The adjoint's kernels.  The gather correlates fields with the kernels mirrored through their centre
+// (taps (-dy, -dx)).  Scale s is stored as the mirrored difference D_s = h_s - h_{s-1} (D_0 = h_0): with
+// c the adjoint field and [.] the selection mask,
+//     sum_s h_s * (c [s* = s]) = sum_s D_s * (c [s* >= s]),
+// so the gather masks one field in place, scale after scale, instead of building a field per scale.
+// The difference is formed in double over the union of the two kernels' boxes (centres aligned) and
+// rounded once.  Same device layout as the forward blob (BlobLayout): run ranges, runs
+// {dy, dx0, len, wofs}, weights as {w, w} pairs with every run padded to an even length, 16 spare taps.
+// ---------------------------------------------------------------------------------------------
+static int build_adjoint_blob(lpaici_kernelset *ks) {
+    const int D = ks->D, S = ks->S, nk = D * S;
+    std::vector<int> begin(nk + 1), rdy, rdx, rlen;
+    std::vector<float> w;
+    for (int d = 0; d < D; d++)
+        for (int s = 0; s < S; s++) {
+            const int k = d * S + s;
+            begin[k] = static_cast<int>(rdy.size());
+            const int kp = s > 0 ? k - 1 : -1;  // the kernel subtracted: h_{s-1}
+            const int hy = std::max(ks->rows[k] / 2, kp >= 0 ? ks->rows[kp] / 2 : 0);
+            const int hx = std::max(ks->cols[k] / 2, kp >= 0 ? ks->cols[kp] / 2 : 0);
+            const int bw = 2 * hx + 1;
+            std::vector<double> box(static_cast<size_t>(2 * hy + 1) * bw, 0.0);  // offset (dy, dx) at (dy+hy, dx+hx)
+            auto add = [&](int kk, double sign) {
+                const float *h = ks->dense_w.data() + ks->off[kk];
+                const int R = ks->rows[kk], Cc = ks->cols[kk];
+                for (int r = 0; r < R; r++)
+                    for (int c = 0; c < Cc; c++)
+                        box[static_cast<size_t>(r - R / 2 + hy) * bw + (c - Cc / 2 + hx)] += sign * h[r * Cc + c];
+            };
+            add(k, 1.0);
+            if (kp >= 0) add(kp, -1.0);
+            // mirrored: tap (my, mx) of the gather kernel is box(-my, -mx)
+            for (int my = -hy; my <= hy; my++) {
+                const double *row = box.data() + static_cast<size_t>(-my + hy) * bw;
+                int first = 1 << 30, last = -(1 << 30);
+                for (int mx = -hx; mx <= hx; mx++)
+                    if (static_cast<float>(row[-mx + hx]) != 0.0f) {
+                        first = std::min(first, mx);
+                        last = std::max(last, mx);
+                    }
+                if (first > last) continue;
+                rdy.push_back(my);
+                rdx.push_back(first);
+                rlen.push_back(last - first + 1);
+                for (int mx = first; mx <= last; mx++) w.push_back(static_cast<float>(row[-mx + hx]));
+            }
+        }
+    begin[nk] = static_cast<int>(rdy.size());
+    const int n_runs = begin[nk];
+    BlobLayout L;
+    L.nk = nk;
+    L.n_runs = n_runs;
+    L.run_word = (nk + 1 + 3) & ~3;
+    L.weight_word = L.run_word + 4 * n_runs;
+    std::vector<int> wofs(n_runs);
+    int n2 = 0;
+    for (int r = 0; r < n_runs; r++) {
+        wofs[r] = n2;
+        n2 += (rlen[r] + 1) & ~1;
+    }
+    L.n_wdup = n2;
+    L.total_words = (L.weight_word + 2 * (n2 + 16) + 3) & ~3;
+    ks->adj_layout = L;
+    ks->adj_blob.assign(L.total_words, 0);
+    for (int k = 0; k <= nk; k++) ks->adj_blob[k] = begin[k];
+    float *wd = reinterpret_cast<float *>(ks->adj_blob.data() + L.weight_word);
+    int wi = 0;
+    for (int r = 0; r < n_runs; r++) {
+        ks->adj_blob[L.run_word + 4 * r + 0] = rdy[r];
+        ks->adj_blob[L.run_word + 4 * r + 1] = rdx[r];
+        ks->adj_blob[L.run_word + 4 * r + 2] = rlen[r];
+        ks->adj_blob[L.run_word + 4 * r + 3] = wofs[r];
+        for (int j = 0; j < rlen[r]; j++, wi++) {
+            wd[2 * (wofs[r] + j)] = w[wi];
+            wd[2 * (wofs[r] + j) + 1] = w[wi];
+        }
+    }
+    return LPAICI_OK;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -113,26 +195,7 @@ static int finish_kernelset(lpaici_kernelset *ks) {
         }
     }
 
-    // adjoint blob: every run mirrored through the kernel centre
-    ks->adj_run_word = (nk + 1 + 3) & ~3;
-    ks->adj_weight_word = ks->adj_run_word + 4 * L.n_runs;
-    const int n_taps = static_cast<int>(ks->run_w.size());
-    ks->adj_blob.assign((ks->adj_weight_word + n_taps + 16 + 3) & ~3, 0);
-    for (int k = 0; k <= nk; k++) ks->adj_blob[k] = ks->blob[k];
-    float *aw = reinterpret_cast<float *>(ks->adj_blob.data() + ks->adj_weight_word);
-    for (int k = 0; k < nk; k++) {
-        int w = ks->k_first_weight[k];
-        for (int r = ks->k_first_run[k]; r < ks->k_first_run[k] + ks->k_num_runs[k]; r++) {
-            const int len = ks->run_len[r];
-            ks->adj_blob[ks->adj_run_word + 4 * r + 0] = -ks->run_row[r];
-            ks->adj_blob[ks->adj_run_word + 4 * r + 1] = -(ks->run_col[r] + len - 1);
-            ks->adj_blob[ks->adj_run_word + 4 * r + 2] = len;
-            ks->adj_blob[ks->adj_run_word + 4 * r + 3] = w;
-            for (int j = 0; j < len; j++) aw[w + j] = ks->run_w[w + len - 1 - j];
-            w += len;
-        }
-    }
-    return LPAICI_OK;
+    return build_adjoint_blob(ks);
 }
 
 int device_blob(const lpaici_kernelset *ks, const int **out) {
@@ -456,6 +519,97 @@ int lpaici_kernelset_load(const char *path, lpaici_kernelset **out) {
     return LPAICI_OK;
 }
 
+int lpaici_kernelset_generate(int num_dirs, int num_scales, const int *scales, int order, int shape,
+                              lpaici_kernelset **out) {
+    if (!scales || !out || num_dirs <= 0 || num_scales <= 0 || order < 0 || order > 4 ||
+        (shape != LPAICI_SHAPE_SECTOR && shape != LPAICI_SHAPE_QUADRANT))
+        return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_kernelset_generate: bad directions, scales, order or shape");
+    *out = nullptr;
+    if (static_cast<long>(num_dirs) * num_scales > kMaxKernels)
+        return set_error(LPAICI_ERR_UNSUPPORTED, "%d x %d kernels; at most %d", num_dirs, num_scales, kMaxKernels);
+    for (int s = 0; s < num_scales; s++)
+        if (scales[s] < 1 || scales[s] > kMaxRadius + 1)
+            return set_error(LPAICI_ERR_INVALID_ARG, "scale %d is %d; 1 .. %d", s, scales[s], kMaxRadius + 1);
+    const double kPi = 3.14159265358979323846;
+    std::vector<float> w;
+    std::vector<int> off, rows, cols;
+    for (int d = 0; d < num_dirs; d++) {
+        const double th = 2.0 * kPi * d / num_dirs, c = std::cos(th), sn = std::sin(th);
+        for (int si = 0; si < num_scales; si++) {
+            const int h = scales[si], R = h - 1, n = 2 * R + 1;
+            // support: pixel (x, y) (y down) has u = x cos + (-y) sin along the direction, v across it
+            std::vector<int> idx;
+            std::vector<double> us;
+            for (int y = -R; y <= R; y++)
+                for (int x = -R; x <= R; x++) {
+                    const double X = x, Y = -y;
+                    const double u = X * c + Y * sn, v = -X * sn + Y * c;
+                    bool in;
+                    if (shape == LPAICI_SHAPE_SECTOR)
+                        in = (x == 0 && y == 0) || (u < h - 0.5 && std::fabs(std::atan2(v, u)) <= kPi / num_dirs + 1e-9);
+                    else
+                        in = u > -0.5 && u < h - 0.5 && v < 0.5 && v > -(h - 0.5);
+                    if (in) {
+                        idx.push_back((y + R) * n + (x + R));
+                        us.push_back(u);
+                    }
+                }
+            // least-squares polynomial in u of order p (at most the distinct u values less one), equal
+            // weights, evaluated at the origin: g_i = sum_q beta_q u_i^q, (sum_i u_i^(j+q)) beta = e_0
+            std::vector<double> distinct = us;
+            std::sort(distinct.begin(), distinct.end());
+            int nu = 0;
+            for (size_t i = 0; i < distinct.size(); i++)
+                if (i == 0 || distinct[i] - distinct[i - 1] > 1e-9) nu++;
+            const int p = std::min(order, nu - 1), m = p + 1;
+            double A[5][6] = {};
+            for (int j = 0; j < m; j++) {
+                for (int q = 0; q < m; q++)
+                    for (const double u : us) A[j][q] += std::pow(u, j + q);
+                A[j][m] = j == 0 ? 1.0 : 0.0;
+            }
+            for (int col = 0; col < m; col++) {  // Gauss-Jordan with partial pivoting
+                int piv = col;
+                for (int r = col + 1; r < m; r++)
+                    if (std::fabs(A[r][col]) > std::fabs(A[piv][col])) piv = r;
+                for (int q = 0; q <= m; q++) std::swap(A[col][q], A[piv][q]);
+                for (int r = 0; r < m; r++) {
+                    if (r == col) continue;
+                    const double f = A[r][col] / A[col][col];
+                    for (int q = col; q <= m; q++) A[r][q] -= f * A[col][q];
+                }
+            }
+            off.push_back(static_cast<int>(w.size()));
+            rows.push_back(n);
+            cols.push_back(n);
+            const size_t base = w.size();
+            w.resize(base + static_cast<size_t>(n) * n, 0.0f);
+            for (size_t i = 0; i < idx.size(); i++) {
+                double g = 0.0;
+                for (int q = 0; q < m; q++) g += A[q][m] / A[q][q] * std::pow(us[i], q);
+                w[base + idx[i]] = static_cast<float>(g);
+            }
+        }
+    }
+    return lpaici_kernelset_create(w.data(), off.data(), rows.data(), cols.data(), num_dirs, num_scales, out);
+}
+
+int lpaici_kernelset_write_text(const lpaici_kernelset *ks, const char *path) {
+    if (!ks || !path) return set_error(LPAICI_ERR_INVALID_ARG, "lpaici_kernelset_write_text: null argument");
+    FILE *f = std::fopen(path, "w");
+    if (!f) return set_error(LPAICI_ERR_FILE, "cannot write %s", path);
+    std::fprintf(f, "%d %d\n", ks->D, ks->S);
+    for (int k = 0; k < ks->D * ks->S; k++) {
+        std::fprintf(f, "%d %d\n", ks->rows[k], ks->cols[k]);
+        const float *h = ks->dense_w.data() + ks->off[k];
+        for (int i = 0; i < ks->rows[k] * ks->cols[k]; i++) std::fprintf(f, "%f ", static_cast<double>(h[i]));
+        std::fprintf(f, "\n");
+    }
+    const bool ok = std::fflush(f) == 0 && !std::ferror(f);
+    std::fclose(f);
+    return ok ? LPAICI_OK : set_error(LPAICI_ERR_FILE, "writing %s failed", path);
+}
+
 int lpaici_kernelset_create(const float *weights, const int *offsets, const int *rows, const int *cols, int num_dirs,
                             int num_scales, lpaici_kernelset **out) {
     if (!weights || !offsets || !rows || !cols || !out || num_dirs <= 0 || num_scales <= 0)
@@ -555,6 +709,8 @@ int lpaici_kernelset_get_info(const lpaici_kernelset *ks, lpaici_kernelset_info_
     info->n_taps = static_cast<int>(ks->run_w.size());
     info->n_runs = static_cast<int>(ks->run_row.size());
     info->radius = ks->radius;
+    info->blob_bytes = static_cast<int>(sizeof(int32_t) * ks->blob.size());
+    info->adjoint_blob_bytes = static_cast<int>(sizeof(int32_t) * ks->adj_blob.size());
     return LPAICI_OK;
 }
 

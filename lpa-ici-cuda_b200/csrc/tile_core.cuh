@@ -58,6 +58,32 @@ __device__ __forceinline__ float2 add2(float2 a, float2 b) {
     return d;
 }
 
+// One tap of the forward: the product rounded, then the sum rounded (bit-exact with the reference).
+struct ExactTap {
+    float2 nz;  // {-0, -0}, read at run time (see prod2)
+    __device__ __forceinline__ float2 operator()(float2 acc, float2 w, float2 x) const {
+        return add2(acc, prod2(w, x, nz));
+    }
+};
+
+// d = a * b + c in each half, rounded on its own (the two halves of fmaf).
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
+        "fma.rn.f32x2 rd, ra, rb, rc;\n\t"
+        "mov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return d;
+}
+
+// One tap as a fused multiply-add, acc + w * x rounded once: the adjoint's gather, and the forward's
+// contracted mode (not bit-exact with the reference).
+struct FmaTap {
+    __device__ __forceinline__ float2 operator()(float2 acc, float2 w, float2 x) const { return fma2(w, x, acc); }
+};
+
 // Smallest odd pitch (in float2) >= need.
 __host__ __device__ inline int tile_pitch2(int need) { return need | 1; }
 
@@ -87,20 +113,22 @@ struct TileGeom {
 __host__ __device__ inline int table_words(int nk) { return (3 * nk + 3) & ~3; }
 
 // One tap column J of a block of Q: window slot (J + Q - 1) % Q receives column k + J + Q - 1, then
-// the Q pixel pairs m accumulate w * column (k + J + m).  Weights come two taps per float4.
+// the Q pixel pairs m accumulate w * column (k + J + m) with the tap operation.  Weights come two taps
+// per float4.
 #define LPAICI_STEP(J)                                                                               \
     {                                                                                                \
         if (((J) & 1) == 0) wv = wq[(J) >> 1];                                                       \
         const float2 w2 = ((J) & 1) ? make_float2(wv.z, wv.w) : make_float2(wv.x, wv.y);             \
         win[((J) + Q - 1) % Q] = src[(J) + Q - 1];                                                   \
-        _Pragma("unroll") for (int m = 0; m < Q; m++) acc[m] = add2(acc[m], prod2(w2, win[((J) + m) % Q], nz)); \
+        _Pragma("unroll") for (int m = 0; m < Q; m++) acc[m] = tap(acc[m], w2, win[((J) + m) % Q]);  \
     }
 
 // The last N (< Q) taps of a run: their window columns and weights are loaded before any of them is
-// used, so the tail pays no load latency per tap.
-template <int Q, int N>
-__device__ __forceinline__ void conv_tail(float2 (&acc)[Q], float2 (&win)[Q], const float2 *__restrict__ src,
-                                          const float4 *__restrict__ wq, float2 nz) {
+// used, so the tail pays no load latency per tap.  Win: a pointer to the run's first column pair, or a
+// window type with the same indexing (the adjoint's masked field).
+template <int Q, int N, class Win, class Tap>
+__device__ __forceinline__ void conv_tail(float2 (&acc)[Q], float2 (&win)[Q], const Win &src,
+                                          const float4 *__restrict__ wq, const Tap &tap) {
     float2 tail[N];
     float4 tw[(N + 1) / 2];
 #pragma unroll
@@ -112,42 +140,41 @@ __device__ __forceinline__ void conv_tail(float2 (&acc)[Q], float2 (&win)[Q], co
         const float2 w2 = (J & 1) ? make_float2(tw[J >> 1].z, tw[J >> 1].w) : make_float2(tw[J >> 1].x, tw[J >> 1].y);
         win[(J + Q - 1) % Q] = tail[J];
 #pragma unroll
-        for (int m = 0; m < Q; m++) acc[m] = add2(acc[m], prod2(w2, win[(J + m) % Q], nz));
+        for (int m = 0; m < Q; m++) acc[m] = tap(acc[m], w2, win[(J + m) % Q]);
     }
 }
 
-template <int Q>
-__device__ __forceinline__ void conv_tail_dispatch(int rem, float2 (&acc)[Q], float2 (&win)[Q],
-                                                   const float2 *__restrict__ src, const float4 *__restrict__ wq,
-                                                   float2 nz) {
+template <int Q, class Win, class Tap>
+__device__ __forceinline__ void conv_tail_dispatch(int rem, float2 (&acc)[Q], float2 (&win)[Q], const Win &src,
+                                                   const float4 *__restrict__ wq, const Tap &tap) {
     if constexpr (Q == 4) {
         switch (rem) {
-            case 1: conv_tail<Q, 1>(acc, win, src, wq, nz); break;
-            case 2: conv_tail<Q, 2>(acc, win, src, wq, nz); break;
-            default: conv_tail<Q, 3>(acc, win, src, wq, nz); break;
+            case 1: conv_tail<Q, 1>(acc, win, src, wq, tap); break;
+            case 2: conv_tail<Q, 2>(acc, win, src, wq, tap); break;
+            default: conv_tail<Q, 3>(acc, win, src, wq, tap); break;
         }
     } else {
         static_assert(Q == 8, "tile configurations use Q = 4 or 8");
         switch (rem) {
-            case 1: conv_tail<Q, 1>(acc, win, src, wq, nz); break;
-            case 2: conv_tail<Q, 2>(acc, win, src, wq, nz); break;
-            case 3: conv_tail<Q, 3>(acc, win, src, wq, nz); break;
-            case 4: conv_tail<Q, 4>(acc, win, src, wq, nz); break;
-            case 5: conv_tail<Q, 5>(acc, win, src, wq, nz); break;
-            case 6: conv_tail<Q, 6>(acc, win, src, wq, nz); break;
-            default: conv_tail<Q, 7>(acc, win, src, wq, nz); break;
+            case 1: conv_tail<Q, 1>(acc, win, src, wq, tap); break;
+            case 2: conv_tail<Q, 2>(acc, win, src, wq, tap); break;
+            case 3: conv_tail<Q, 3>(acc, win, src, wq, tap); break;
+            case 4: conv_tail<Q, 4>(acc, win, src, wq, tap); break;
+            case 5: conv_tail<Q, 5>(acc, win, src, wq, tap); break;
+            case 6: conv_tail<Q, 6>(acc, win, src, wq, tap); break;
+            default: conv_tail<Q, 7>(acc, win, src, wq, tap); break;
         }
     }
 }
 
-// acc[m] += sum_{j < len} {w_j, w_j} * src[m + j], tap by tap in order, for the Q pixel pairs.
+// acc[m] = tap(acc[m], {w_j, w_j}, src[m + j]) for j < len, tap by tap in order, for the Q pixel pairs.
 // src: the run's first column in T8 (row already chosen); wq: the run's duplicated weights as
 // float4 {w_2i, w_2i, w_2i+1, w_2i+1}.
 // The last len % Q taps go to a tail of exactly that many taps (conv_tail): one warp-uniform
 // dispatch, no test per tap.  src and wq advance with the taps, so every load has a constant offset.
-template <int Q>
-__device__ __forceinline__ void conv_run(float2 (&acc)[Q], const float2 *__restrict__ src,
-                                         const float4 *__restrict__ wq, int len, float2 nz) {
+template <int Q, class Win, class Tap>
+__device__ __forceinline__ void conv_run(float2 (&acc)[Q], Win src, const float4 *__restrict__ wq, int len,
+                                         const Tap &tap) {
     float2 win[Q];
     float4 wv;
 #pragma unroll
@@ -158,7 +185,7 @@ __device__ __forceinline__ void conv_run(float2 (&acc)[Q], const float2 *__restr
         for (int J = 0; J < Q; J++) LPAICI_STEP(J)
     }
     // rem: 0 .. Q-1, warp-uniform: one dispatch to a tail of exactly rem taps
-    if (rem > 0) conv_tail_dispatch<Q>(rem, acc, win, src, wq, nz);
+    if (rem > 0) conv_tail_dispatch<Q>(rem, acc, win, src, wq, tap);
 }
 #undef LPAICI_STEP
 
@@ -239,7 +266,7 @@ using ScaleBits = typename std::conditional<(8 * Q <= 32), unsigned, unsigned lo
 // mask, its updates simply never accept again.  Scale 0 is always accepted (lo = -inf, hi = +inf), so
 // the index is the count of accepted scales after it.  Warp-uniform scale loop; it ends when every
 // valid pixel of the warp has stopped.
-template <int Q>
+template <int Q, bool Fused>
 __device__ __forceinline__ void direction_sweep(int d, int S, unsigned valid, const float2 *lane_tile,
                                                 const int *s_blob, const int4 *s_runs, const float4 *s_wq,
                                                 const float *s_thr, float2 nz, float2 (&best)[Q], ScaleBits<Q> &sidx) {
@@ -265,7 +292,10 @@ __device__ __forceinline__ void direction_sweep(int d, int S, unsigned valid, co
 #pragma unroll(Q == 4 ? 2 : 1)
         for (int r = rb; r < re; r++) {
             const int4 run = s_runs[r];  // (tile offset, len, float4 weight index): see stage_blob
-            conv_run<Q>(acc, lane_tile + run.x, s_wq + run.z, run.y, nz);
+            if constexpr (Fused)
+                conv_run<Q>(acc, lane_tile + run.x, s_wq + run.z, run.y, FmaTap{});
+            else
+                conv_run<Q>(acc, lane_tile + run.x, s_wq + run.z, run.y, ExactTap{nz});
         }
         const float thr = s_thr[k];
         const ScaleBits<Q> step = s > 0 ? 1 : 0;
@@ -292,7 +322,7 @@ __device__ __forceinline__ void direction_sweep(int d, int S, unsigned valid, co
 }
 
 // The forward sweep of one tile (tile in shared memory, block-synchronised).
-template <int WX, int Q>
+template <int WX, int Q, bool Fused = false>
 __device__ __forceinline__ void sweep_tile(const ImageArgs &img, int x0, int y0, int D, int S, const TileGeom &g,
                                            const int *s_blob, int run_word, int weight_word, const float *s_tab,
                                            const float2 *s_tile, float neg_zero) {
@@ -316,7 +346,7 @@ __device__ __forceinline__ void sweep_tile(const ImageArgs &img, int x0, int y0,
     for (int d = 0; d < D; d++) {
         float2 best[Q];
         ScaleBits<Q> sidx;
-        direction_sweep<Q>(d, S, valid, lane_tile, s_blob, s_runs, s_wq, s_thr, nz, best, sidx);
+        direction_sweep<Q, Fused>(d, S, valid, lane_tile, s_blob, s_runs, s_wq, s_thr, nz, best, sidx);
 #pragma unroll
         for (int m = 0; m < Q; m++) {
             const float2 r = make_float2(s_rvar[d * S + static_cast<int>((sidx >> (8 * m)) & 15)],

@@ -52,7 +52,7 @@ class LpaIciError(RuntimeError):
 
 class KernelSetInfo(C.Structure):
     _fields_ = [("num_dirs", C.c_int), ("num_scales", C.c_int), ("dense_size", C.c_int), ("n_taps", C.c_int),
-                ("n_runs", C.c_int), ("radius", C.c_int)]
+                ("n_runs", C.c_int), ("radius", C.c_int), ("blob_bytes", C.c_int), ("adjoint_blob_bytes", C.c_int)]
 
 
 class Image(C.Structure):
@@ -100,6 +100,9 @@ _SIGS = {
     "lpaici_set_tile_config": ([_vp, _i], _i),
     "lpaici_backward": ([_vp, _vp, _i, _vp, _i, _vp, _i, _i, _i, _f, _f, _vp], _i),
     "lpaici_backward_noalloc": ([_vp, _vp, _i, _vp, _i, _vp, _i, _i, _i, _f, _f, _vp], _i),
+    "lpaici_forward_ffma": ([_vp, _vp, _i, _vp, _i, _i, _i, _f, _f, _vp, _vp], _i),
+    "lpaici_kernelset_generate": ([_i, _i, _ip, _i, _i, C.POINTER(_vp)], _i),
+    "lpaici_kernelset_write_text": ([_vp, C.c_char_p], _i),
     "lpaici_trim_workspace": ([], _i),
     "lpaici_forward_channels": ([_vp, _vp, _i, _vp, _i, _i, _i, _i, _f, _f, _vp], _i),
     "lpaici_adjoint_state_bytes": ([_vp, _i, _i], C.c_size_t),
@@ -177,6 +180,21 @@ class KernelSet:
         _check(_lib.lpaici_kernelset_create(_fptr(w), _iptr(o), _iptr(r), _iptr(c), num_dirs, num_scales,
                                             C.byref(h)), "lpaici_kernelset_create")
         return cls(h.value)
+
+    @classmethod
+    def generate(cls, num_dirs: int, scales, order: int = 0, shape: str = "sector") -> "KernelSet":
+        """Directional LPA kernels from their definition (lpaici_kernelset_generate): `shape` "sector"
+        or "quadrant", polynomial `order` along the direction, one kernel per scale in `scales`."""
+        sc = np.ascontiguousarray(scales, np.int32)
+        code = {"sector": 0, "quadrant": 1}[shape]
+        h = C.c_void_p()
+        _check(_lib.lpaici_kernelset_generate(num_dirs, sc.size, _iptr(sc), order, code, C.byref(h)),
+               "lpaici_kernelset_generate")
+        return cls(h.value)
+
+    def save_text(self, path: str) -> None:
+        """The reference's text kernel format (lpaici_kernelset_write_text)."""
+        _check(_lib.lpaici_kernelset_write_text(self._h, path.encode()), "lpaici_kernelset_write_text")
 
     def save(self, path: str) -> None:
         """Writes the binary tap-list file that load() reads back (lpaici_kernelset_save)."""
@@ -279,10 +297,11 @@ def _check_image(t, name: str):
 
 
 def forward(ks: KernelSet, noisy, sigma: float, gamma: float, out=None, scale_map: bool | object = False,
-            variances: Optional[np.ndarray] = None):
+            variances: Optional[np.ndarray] = None, ffma: bool = False):
     """Denoises one image on its device.  Returns out, or (out, scale_map uint8 [D, H, W]) when scale_map
     is True (or a preallocated tensor).  With `variances` (D*S floats) the reference's caller-supplied
-    variances are used instead of sigma."""
+    variances are used instead of sigma.  ffma=True: lpaici_forward_ffma (fused multiply-adds, not
+    bit-exact with the reference)."""
     import torch
 
     _check_image(noisy, "noisy")
@@ -297,7 +316,14 @@ def forward(ks: KernelSet, noisy, sigma: float, gamma: float, out=None, scale_ma
         smap = scale_map
     sp = C.c_void_p(smap.data_ptr()) if smap is not None else None
     with torch.cuda.device(noisy.device):
-        if variances is None:
+        if ffma:
+            if variances is not None:
+                raise ValueError("ffma=True takes sigma, not variances")
+            rc = _lib.lpaici_forward_ffma(ks.handle, C.c_void_p(noisy.data_ptr()), noisy.stride(0),
+                                          C.c_void_p(out.data_ptr()), out.stride(0), W, H, sigma, gamma, sp,
+                                          _stream(torch))
+            _check(rc, "lpaici_forward_ffma")
+        elif variances is None:
             rc = _lib.lpaici_forward(ks.handle, C.c_void_p(noisy.data_ptr()), noisy.stride(0),
                                      C.c_void_p(out.data_ptr()), out.stride(0), W, H, sigma, gamma, sp, _stream(torch))
             _check(rc, "lpaici_forward")

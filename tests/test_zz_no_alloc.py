@@ -95,18 +95,10 @@ def _r256(n: int) -> int:
 
 
 def _scratch_need(ks, W: int, H: int) -> int:
-    """Bytes lpaici_backward_noalloc needs: the layout of kernelset.cpp's two device blobs (int words:
-    run ranges padded to 4, 4 per run, then {w, w} per tap with runs padded to even length and 16 spare
-    taps / one float per tap and 16 spare), each 256-rounded, then D*W*H selection bytes (256-rounded)
-    and W*H floats of 1/den."""
-    r = ks.runs()
-    nk = ks.D * ks.S
-    head = (nk + 1 + 3) & ~3
-    run_words = 4 * len(r.run_len)
-    n2 = int(sum((int(n) + 1) & ~1 for n in r.run_len))
-    blob_words = (head + run_words + 2 * (n2 + 16) + 3) & ~3
-    adj_words = (head + run_words + int(r.run_len.sum()) + 16 + 3) & ~3
-    return _r256(4 * blob_words) + _r256(4 * adj_words) + _r256(ks.D * W * H) + 4 * W * H
+    """Bytes lpaici_backward_noalloc needs: the two device kernel blobs (sizes from the kernel set's
+    info), each 256-rounded, then D*W*H selection bytes (256-rounded) and W*H floats of 1/den."""
+    info = ks.info
+    return _r256(info.blob_bytes) + _r256(info.adjoint_blob_bytes) + _r256(ks.D * W * H) + 4 * W * H
 
 
 def _largest_rows(ks, W: int) -> int:
