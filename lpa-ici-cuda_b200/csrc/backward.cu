@@ -53,8 +53,8 @@ struct GatherShape {
     static constexpr int kGroupThreads = 32 * kGatherWX * WY;
     static constexpr int kThreads = kGatherG * kGroupThreads;
 };
-// Tile heights the host can choose (the tallest whose fields and kernels fit in shared memory).
-constexpr int kGatherWYs[] = {4, 3, 2, 1};
+// Tile heights the host can choose (the tallest whose fields and kernels fit in shared memory), four of them.
+constexpr int kGatherWYs[4] = {4, 3, 2, 1};
 
 // Field geometry: rows th + 2R, pitch 1 mod 8 and >= tw + 2R + Q (a margin no load reaches).
 struct GatherGeom {
@@ -260,26 +260,32 @@ __global__ void __launch_bounds__(GatherShape<WY>::kThreads, 1)
 
 namespace {
 
-template <int WY>
-const void *gather_fn() {
-    return reinterpret_cast<const void *>(lpaici_adjoint_gather_kernel<WY>);
-}
+// The gather kernel of tile height index I .. 3 whose WY is wy (null when none is).
+template <int I>
 const void *gather_fn(int wy) {
-    switch (wy) {
-        case 4: return gather_fn<4>();
-        case 3: return gather_fn<3>();
-        case 2: return gather_fn<2>();
-        default: return gather_fn<1>();
+    if constexpr (I < 4) {
+        if (wy == kGatherWYs[I]) return reinterpret_cast<const void *>(lpaici_adjoint_gather_kernel<kGatherWYs[I]>);
+        return gather_fn<I + 1>(wy);
+    } else {
+        return nullptr;
+    }
+}
+
+template <int I>
+bool gather_launch_at(const GatherArgs &ga, int wy, unsigned grid, size_t smem, cudaStream_t stream) {
+    if constexpr (I < 4) {
+        constexpr int WY = kGatherWYs[I];
+        if (wy != WY) return gather_launch_at<I + 1>(ga, wy, grid, smem, stream);
+        lpaici_adjoint_gather_kernel<WY><<<grid, GatherShape<WY>::kThreads, smem, stream>>>(ga);
+        return true;
+    } else {
+        return false;
     }
 }
 
 int gather_launch(const GatherArgs &ga, int wy, unsigned grid, size_t smem, cudaStream_t stream) {
-    switch (wy) {
-        case 4: lpaici_adjoint_gather_kernel<4><<<grid, GatherShape<4>::kThreads, smem, stream>>>(ga); break;
-        case 3: lpaici_adjoint_gather_kernel<3><<<grid, GatherShape<3>::kThreads, smem, stream>>>(ga); break;
-        case 2: lpaici_adjoint_gather_kernel<2><<<grid, GatherShape<2>::kThreads, smem, stream>>>(ga); break;
-        default: lpaici_adjoint_gather_kernel<1><<<grid, GatherShape<1>::kThreads, smem, stream>>>(ga); break;
-    }
+    if (!gather_launch_at<0>(ga, wy, grid, smem, stream))
+        return set_error(LPAICI_ERR_INVALID_ARG, "adjoint gather: no kernel for tile height %d", wy);
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? LPAICI_OK : cuda_error(e, "adjoint gather launch");
 }
@@ -354,7 +360,7 @@ int gather_setup(const lpaici_kernelset *ks, const int *adj_blob, GatherArgs *ga
         }
         ga->drect[d] = u;
     }
-    cudaError_t e = cudaFuncSetAttribute(gather_fn(*wy), cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(gather_fn<0>(*wy), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(*smem));
     return e == cudaSuccess ? LPAICI_OK : cuda_error(e, "adjoint gather attributes");
 }
