@@ -490,6 +490,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         plan.close()
         extra["batched_one_image"] = {"size": size, "value": px / (np.mean(b_ms) * 1e-3) / 1e6,
                                       "plain": value, "unit": UNIT, "graph": True, "bit_equal_to_plain": bool(same)}
+        # work rate (algorithmic taps per second) of the 64-image batch against the plain 4096^2 launch:
+        # its images carry other sigmas, gammas and sizes, hence other taps per pixel
+        extra["batched"]["work_rate_over_plain"] = extra["batched"]["taps_per_s"] / (taps / (ms_step * 1e-3))
         extra["ffma"] = run_ffma(torch, lpaici, ks, x, out, clean, taps, peak, args, flush)
         ref_gpu = reference_gpu_v4_1(clean, noisy_h, out.cpu().numpy(), min(args.steps, 3))
         if "value" in ref_gpu:
@@ -593,6 +596,13 @@ def run_extras(torch, lpaici, ks, args, flush) -> dict:
     p_ms = time_launches(torch, plain, steps, 1, flush)
     same = all(torch.equal(a.view(torch.int32), b.view(torch.int32)) for a, b in zip(outs, singles))
     batch.close()
+    # the batch's algorithmic taps (its sigmas and gammas differ from the benchmark image's), so that its
+    # work rate can be set beside the plain launch's
+    batch_taps = 0.0
+    for x, s, g in zip(xs, sig, gam):
+        _, sm = lpaici.forward(ks, x, float(s), float(g), scale_map=True)
+        batch_taps += algorithmic_taps(torch, ks, sm)
+        del sm
     del xs, outs, singles
 
     # adjoint: 8 x 1024^2, sigma 20/255, gamma 2, g ~ N(0, 1)
@@ -645,7 +655,9 @@ def run_extras(torch, lpaici, ks, args, flush) -> dict:
     return {
         "batched": {"images": n, "mpix": total_px / 1e6, "value": total_px / (np.mean(b_ms) * 1e-3) / 1e6,
                     "plain_same_images": total_px / (np.mean(p_ms) * 1e-3) / 1e6, "unit": UNIT,
-                    "graph": True, "bit_equal_to_plain": bool(same)},
+                    "graph": True, "bit_equal_to_plain": bool(same),
+                    "algorithmic_taps_per_px": batch_taps / total_px,
+                    "taps_per_s": batch_taps / (np.mean(b_ms) * 1e-3)},
         "adjoint": {"images": m, "size": 1024, "unit": UNIT,
                     "value": m * 1024 * 1024 / (np.mean(ab_ms) * 1e-3) / 1e6,
                     "forward_same_images": m * 1024 * 1024 / (np.mean(fb_ms) * 1e-3) / 1e6,
@@ -741,7 +753,13 @@ def run_profile(args) -> None:
     gamma = 1.5 if gauss else GAMMA
     if args.tile_config >= 0:
         ks.set_tile_config(args.tile_config)
-    if args.profile == "batched":  # the 64-image plan of the batched benchmark, one launch per step
+    if args.profile == "batched_one":  # a batched plan over the one --size image, one launch per step
+        _, noisy_h = bench_image(args.size, SEED, sigma)
+        xs = [torch.from_numpy(noisy_h).cuda()]
+        outs = [torch.empty_like(xs[0])]
+        plan = lpaici.Batch(ks, xs, outs, [sigma], [gamma], use_graph=True)
+        op = plan.run
+    elif args.profile == "batched":  # the 64-image plan of the batched benchmark, one launch per step
         from lpaici.synth import mixed_batch
 
         spec = mixed_batch(64, SEED)
@@ -781,7 +799,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--size", type=int, default=SIZE, help="image side (profiling runs use a smaller case)")
     ap.add_argument("--tile-config", type=int, default=-1, help="fixed tile configuration instead of autotuning")
-    ap.add_argument("--profile", choices=["forward", "ffma", "adjoint", "batched"], default=None,
+    ap.add_argument("--profile", choices=["forward", "ffma", "adjoint", "batched", "batched_one"], default=None,
                     help="run only this operation on one --size image, or the 64-image batched plan (for "
                          "profiler captures; no bench line)")
     ap.add_argument("--kernels", choices=["sym", "gauss_m2"], default="sym",

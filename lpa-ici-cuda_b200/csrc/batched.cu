@@ -7,7 +7,9 @@
 // persistent loop (measured: a persistent grid pulling items from an atomic counter kept its
 // 768-thread instances at the 80-register limit and ran 2-2.5 % slower).  There is no inter-CTA
 // waiting of any kind.  With use_graph the launch is captured once into a CUDA graph and replayed
-// by lpaici_batch_run.
+// by lpaici_batch_run.  A plan of one image launches the single-image kernel instead (image and tables
+// as launch parameters): there are no small-image tails to fill, and the queue decode would cost a
+// little per CTA.
 // No reference counterpart: the reference denoises one image per process
 // (src/v4_1_lpa_ici_2D_sparse_shared.cu:365-530).
 #include <algorithm>
@@ -140,11 +142,18 @@ struct lpaici_batch {
     bool use_graph = false;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    // a plan of one image runs the single-image kernel (image and tables as launch parameters, no queue
+    // to decode): one image has no small-image tails for the queue to fill
+    bool single = false;
+    ImageArgs img{};
+    KernelTables tab{};
+    int config = 0;
 };
 
 namespace lpaici {
 
 int batch_plan_enqueue(lpaici_batch *b, cudaStream_t stream) {
+    if (b->single) return launch_forward(nullptr, b->img, b->tab, b->config, stream);
     void *params[] = {&b->args};
     const cudaError_t e = cudaLaunchKernel(b->info.fn, dim3(b->grid), dim3(b->info.threads), params, b->info.smem, stream);
     if (e != cudaSuccess) return cuda_error(e, "batched launch");
@@ -269,6 +278,23 @@ int batch_plan_create(const lpaici_kernelset *ks, const BatchSpec *specs, int n,
                                 : set_error(LPAICI_ERR_UNSUPPORTED, "batched kernel does not fit on an SM");
     }
     b->grid = b->args.n_items;  // one CTA per queue item
+    if (n == 1) {
+        const BatchSpec &im = specs[0];
+        b->single = true;
+        b->config = config;
+        b->img.in = im.noisy;
+        b->img.out = im.out;
+        b->img.smap = im.smap;
+        b->img.rden = im.rden;
+        b->img.W = im.width;
+        b->img.in_h = im.height;
+        b->img.in_pitch = im.noisy_pitch;
+        b->img.out_pitch = im.out_pitch;
+        b->img.row_begin = 0;
+        b->img.rows_out = im.height;
+        fill_tables(ks, nullptr, im.sigma, im.gamma, &b->tab);
+        b->tab.blob = blob;
+    }
 
     b->use_graph = use_graph;
     if (b->use_graph) {
