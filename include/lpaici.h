@@ -148,8 +148,8 @@ int lpaici_forward(const lpaici_kernelset *ks, const float *d_noisy, int noisy_p
 /* lpaici_forward with every tap computed as one fused multiply-add (product and sum rounded once)
  * instead of a separately rounded product and sum: faster, and NOT bit-exact with the reference,
  * whose CPU build rounds both.  The selected scales can differ where an interval test is a tie at
- * FP32 rounding, which moves that pixel's output by up to about 1e-3 (measured figures in DESIGN.md);
- * everywhere else the output differs from lpaici_forward's by a few ULP.  Same arguments and errors as
+ * FP32 rounding, which moves that pixel's output by up to about 1e-2 (4096^2 benchmark image: 70 of
+ * 16.8 M pixels carry a flipped scale, 64 move by more than 1e-4, at most 1.07e-2); everywhere else the output differs from lpaici_forward's by a few ULP.  Same arguments and errors as
  * lpaici_forward.  No counterpart in the reference (whose GPU builds let the compiler contract some of
  * its multiply-adds). */
 int lpaici_forward_ffma(const lpaici_kernelset *ks, const float *d_noisy, int noisy_pitch, float *d_denoised,
