@@ -490,6 +490,26 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         plan.close()
         extra["batched_one_image"] = {"size": size, "value": px / (np.mean(b_ms) * 1e-3) / 1e6,
                                       "plain": value, "unit": UNIT, "graph": True, "bit_equal_to_plain": bool(same)}
+        # four images of the benchmark's size, sigma and gamma as one plan (one launch, a grid layer per
+        # image) beside the same four as plain calls
+        xs4 = [x] + [torch.from_numpy(bench_image(size, SEED + k, SIGMA)[1]).cuda() for k in (1, 2, 3)]
+        outs4 = [torch.empty_like(v) for v in xs4]
+        plain4 = [torch.empty_like(v) for v in xs4]
+        plan4 = lpaici.Batch(ks, xs4, outs4, [SIGMA] * 4, [GAMMA] * 4, use_graph=True)
+        b4_ms = time_launches(torch, plan4.run, args.steps, 1, flush)
+
+        def plain_four():
+            for v, o in zip(xs4, plain4):
+                lpaici.forward(ks, v, SIGMA, GAMMA, out=o)
+
+        p4_ms = time_launches(torch, plain_four, args.steps, 1, flush)
+        same4 = all(torch.equal(a.view(torch.int32), b.view(torch.int32)) for a, b in zip(outs4, plain4))
+        plan4.close()
+        extra["batched_four_images"] = {"size": size, "images": 4, "value": 4 * px / (np.mean(b4_ms) * 1e-3) / 1e6,
+                                        "plain_same_images": 4 * px / (np.mean(p4_ms) * 1e-3) / 1e6, "unit": UNIT,
+                                        "graph": True, "bit_equal_to_plain": bool(same4),
+                                        "how": "one launch of the single-image kernel with a grid layer per image"}
+        del xs4, outs4, plain4
         # work rate (algorithmic taps per second) of the 64-image batch against the plain 4096^2 launch:
         # its images carry other sigmas, gammas and sizes, hence other taps per pixel
         extra["batched"]["work_rate_over_plain"] = extra["batched"]["taps_per_s"] / (taps / (ms_step * 1e-3))

@@ -202,7 +202,9 @@ typedef struct lpaici_batch lpaici_batch;
 /* Plans a batch: orders all images' tiles largest-work-first into one work queue, uploads the
  * per-image descriptors (pointers, sizes, variances, thresholds) to device memory owned by the plan
  * and, with use_graph, captures the launch on `stream`.  The image pointers are baked in: rerun
- * the plan whenever their contents change, re-plan when the pointers change.  No reference
+ * the plan whenever their contents change, re-plan when the pointers change.  A plan of one image,
+ * or of up to 64 images that share size, pitches, sigma and gamma, launches the single-image kernel
+ * instead (one grid layer per image, no queue); the results are the same bit for bit.  No reference
  * counterpart (the reference denoises one image per process). */
 int lpaici_batch_create(const lpaici_kernelset *ks, const lpaici_image *images, int n,
                         const lpaici_batch_options *opts, lpaici_stream_t stream, lpaici_batch **out);

@@ -9,7 +9,8 @@
 // waiting of any kind.  With use_graph the launch is captured once into a CUDA graph and replayed
 // by lpaici_batch_run.  A plan of one image launches the single-image kernel instead (image and tables
 // as launch parameters): there are no small-image tails to fill, and the queue decode would cost a
-// little per CTA.
+// little per CTA.  A plan of up to kMaxMultiImages images of one size, pitch, sigma and gamma launches
+// that kernel once with a grid layer per image (lpaici_forward_multi_kernel).
 // No reference counterpart: the reference denoises one image per process
 // (src/v4_1_lpa_ici_2D_sparse_shared.cu:365-530).
 #include <algorithm>
@@ -145,6 +146,12 @@ struct lpaici_batch {
     // a plan of one image runs the single-image kernel (image and tables as launch parameters, no queue
     // to decode): one image has no small-image tails for the queue to fill
     bool single = false;
+    // a plan of 2 .. kMaxMultiImages images of one size, pitch, sigma and gamma runs the single-image kernel
+    // once with a grid layer per image (lpaici_forward_multi_kernel): no queue to decode, and each image's
+    // CTAs fill the SMs the previous image's last wave leaves idle
+    bool multi = false;
+    int n_multi = 0;
+    MultiImages mi{};
     ImageArgs img{};
     KernelTables tab{};
     int config = 0;
@@ -154,6 +161,7 @@ namespace lpaici {
 
 int batch_plan_enqueue(lpaici_batch *b, cudaStream_t stream) {
     if (b->single) return launch_forward(nullptr, b->img, b->tab, b->config, stream);
+    if (b->multi) return launch_forward_multi(b->img, b->tab, b->mi, b->n_multi, b->config, stream);
     void *params[] = {&b->args};
     const cudaError_t e = cudaLaunchKernel(b->info.fn, dim3(b->grid), dim3(b->info.threads), params, b->info.smem, stream);
     if (e != cudaSuccess) return cuda_error(e, "batched launch");
@@ -278,9 +286,25 @@ int batch_plan_create(const lpaici_kernelset *ks, const BatchSpec *specs, int n,
                                 : set_error(LPAICI_ERR_UNSUPPORTED, "batched kernel does not fit on an SM");
     }
     b->grid = b->args.n_items;  // one CTA per queue item
-    if (n == 1) {
+    bool one_size = n >= 2 && n <= kMaxMultiImages;
+    for (int i = 1; one_size && i < n; i++) {
+        const BatchSpec &a0 = specs[0], &ai = specs[i];
+        one_size = ai.width == a0.width && ai.height == a0.height && ai.noisy_pitch == a0.noisy_pitch &&
+                   ai.out_pitch == a0.out_pitch && ai.sigma == a0.sigma && ai.gamma == a0.gamma &&
+                   (ai.out == nullptr) == (a0.out == nullptr) && (ai.smap == nullptr) == (a0.smap == nullptr) &&
+                   (ai.rden == nullptr) == (a0.rden == nullptr);
+    }
+    if (n == 1 || one_size) {
         const BatchSpec &im = specs[0];
-        b->single = true;
+        b->single = n == 1;
+        b->multi = one_size;
+        b->n_multi = one_size ? n : 0;
+        for (int i = 0; one_size && i < n; i++) {
+            b->mi.in[i] = specs[i].noisy;
+            b->mi.out[i] = specs[i].out;
+            b->mi.smap[i] = specs[i].smap;
+            b->mi.rden[i] = specs[i].rden;
+        }
         b->config = config;
         b->img.in = im.noisy;
         b->img.out = im.out;

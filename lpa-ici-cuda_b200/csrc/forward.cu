@@ -33,7 +33,61 @@ __global__ void __launch_bounds__(32 * WX * WY, 1)
                              tab.neg_zero);
 }
 
+// Several images of one size, pitch, sigma and gamma in one launch (a batched plan of such images):
+// grid layer z is image z, whose buffers replace img's; everything else is the single-image kernel.  The
+// CTAs of image z + 1 fill the SMs image z's last wave leaves idle.  No counterpart in the reference.
+template <int WX, int WY, int Q>
+__global__ void __launch_bounds__(32 * WX * WY, 1)
+    lpaici_forward_multi_kernel(const __grid_constant__ ImageArgs img, const __grid_constant__ KernelTables tab,
+                                const __grid_constant__ MultiImages mi) {
+    using Shape = TileShape<WX, WY, Q>;
+    extern __shared__ __align__(16) int smem[];
+    const int nk = tab.D * tab.S;
+    int *s_blob = smem;
+    float *s_tab = reinterpret_cast<float *>(smem + tab.blob_words);
+    float2 *s_tile = reinterpret_cast<float2 *>(smem + tab.blob_words + table_words(nk));
+    const TileGeom g = TileGeom::make(Shape::kTileW, Shape::kTileH, tab.R, Q);
+    const int x0 = blockIdx.x * Shape::kTileW, y0 = blockIdx.y * Shape::kTileH;
+    ImageArgs im = img;
+    im.in = mi.in[blockIdx.z];
+    im.out = mi.out[blockIdx.z];
+    im.smap = mi.smap[blockIdx.z];
+    im.rden = mi.rden[blockIdx.z];
+
+    stage_blob(s_blob, tab.blob, tab.blob_words, tab.run_word, tab.weight_word, g.pitch2);
+    stage_tables(s_tab, tab.var, tab.thr, nk);
+    load_tile(s_tile, im, x0, y0, g);
+    __syncthreads();
+    sweep_tile<WX, Q, false>(im, x0, y0, tab.D, tab.S, g, s_blob, tab.run_word, tab.weight_word, s_tab, s_tile,
+                             tab.neg_zero);
+}
+
 namespace {
+
+template <int WX, int WY, int Q>
+int launch_multi_cfg(const ImageArgs &img, const KernelTables &tab, const MultiImages &mi, int n,
+                     cudaStream_t stream) {
+    using Shape = TileShape<WX, WY, Q>;
+    const TileGeom g = TileGeom::make(Shape::kTileW, Shape::kTileH, tab.R, Q);
+    const int nk = tab.D * tab.S;
+    const size_t smem = sizeof(int) * (tab.blob_words + table_words(nk)) + g.tile_bytes();
+    auto kern = lpaici_forward_multi_kernel<WX, WY, Q>;
+    int dev = 0, max_optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (smem > static_cast<size_t>(max_optin))
+        return set_error(LPAICI_ERR_UNSUPPORTED, "forward tile needs %zu B of shared memory, device allows %d", smem,
+                         max_optin);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute(forward, several images)");
+    const dim3 grid((img.W + Shape::kTileW - 1) / Shape::kTileW, (img.rows_out + Shape::kTileH - 1) / Shape::kTileH,
+                    n);
+    if (grid.y > 65535u) return set_error(LPAICI_ERR_UNSUPPORTED, "image too tall: %d rows", img.rows_out);
+    kern<<<grid, Shape::kThreads, smem, stream>>>(img, tab, mi);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_error(e, "forward launch (several images)");
+    return LPAICI_OK;
+}
 
 template <int WX, int WY, int Q, bool Fused>
 int launch_cfg(const ImageArgs &img, const KernelTables &tab, cudaStream_t stream) {
@@ -112,6 +166,22 @@ size_t config_smem(int config, int blob_words, int nk, int R) {
         default: return ~size_t(0);
     }
 #undef LPAICI_SMEM_CASE
+}
+
+int launch_forward_multi(const ImageArgs &img, const KernelTables &tab, const MultiImages &mi, int n, int config,
+                         cudaStream_t stream) {
+    if (tab.S > kMaxScales)
+        return set_error(LPAICI_ERR_UNSUPPORTED, "%d scales per direction; the kernels support at most %d", tab.S,
+                         kMaxScales);
+    if (n < 1 || n > kMaxMultiImages)
+        return set_error(LPAICI_ERR_INVALID_ARG, "%d images in one launch; at most %d", n, kMaxMultiImages);
+#define LPAICI_MULTI_CASE(idx, WX, WY, Q) \
+    case idx: return launch_multi_cfg<WX, WY, Q>(img, tab, mi, n, stream);
+    switch (config) {
+        LPAICI_TILE_CONFIGS(LPAICI_MULTI_CASE)
+        default: return set_error(LPAICI_ERR_INVALID_ARG, "tile config %d out of range", config);
+    }
+#undef LPAICI_MULTI_CASE
 }
 
 int launch_forward(const lpaici_kernelset *ks, const ImageArgs &img, const KernelTables &tab, int config,

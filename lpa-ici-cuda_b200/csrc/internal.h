@@ -57,6 +57,16 @@ struct KernelTables {
     float thr[kMaxKernels];
 };
 
+// Buffers of the images of a one-size batched plan (lpaici_forward_multi_kernel): image z's input,
+// output, scale maps and 1/den (the last three may be null, as in ImageArgs).
+constexpr int kMaxMultiImages = 64;
+struct MultiImages {
+    const float *in[kMaxMultiImages];
+    float *out[kMaxMultiImages];
+    uint8_t *smap[kMaxMultiImages];
+    float *rden[kMaxMultiImages];
+};
+
 int set_error(int code, const char *fmt, ...);
 int cuda_error(cudaError_t e, const char *what);
 // The checks every adjoint entry point makes before any copy or launch: sigma and gamma finite and
@@ -113,6 +123,9 @@ void fill_tables(const lpaici_kernelset *ks, const float *var_or_null, float sig
 // bit-exact with the reference: lpaici_forward_ffma).
 int launch_forward(const lpaici_kernelset *ks, const ImageArgs &img, const KernelTables &tab, int config,
                    cudaStream_t stream, bool fused = false);
+// n images of img's size, pitches and tables (tab) in one launch, their buffers in mi.
+int launch_forward_multi(const ImageArgs &img, const KernelTables &tab, const MultiImages &mi, int n, int config,
+                         cudaStream_t stream);
 // Bytes of shared memory tile configuration `config` needs for a kernel set.
 size_t config_smem(int config, int blob_words, int nk, int R);
 // The autotuned configuration of ks on the current device, else the first one that fits.

@@ -81,3 +81,33 @@ def test_one_shot_and_errors(setup):
         assert torch.equal(o.view(torch.int32), s.view(torch.int32))
     with pytest.raises(lpaici.LpaIciError):
         lpaici.Batch(ks, imgs[:2], outs[:2], [0.1, -1.0], [2.0, 2.0])
+
+
+@pytest.mark.parametrize("config", [-1] + list(range(lpaici.lib().lpaici_num_tile_configs())))
+def test_one_size_plan(setup, config):
+    """A plan of images of one size, pitch, sigma and gamma runs the single-image kernel once with a grid
+    layer per image: every image equals its single-image call bit for bit, and the scale maps and outputs
+    equal the oracle's."""
+    torch, ks, ko, imgs, sig, gam, singles = setup
+    s, g = sig[5], gam[5]
+    xs = [torch.from_numpy(lpaici.add_noise(lpaici.synth_image(173, 131, 2000 + i), s, 77 + i)).cuda()
+          for i in range(5)]
+    ref = [lpaici.forward(ks, x, s, g) for x in xs]
+    outs = [torch.full_like(x, float("nan")) for x in xs]
+    maps = [torch.empty((ks.D,) + tuple(x.shape), dtype=torch.uint8, device="cuda") for x in xs]
+    b = lpaici.Batch(ks, xs, outs, [s] * len(xs), [g] * len(xs), use_graph=config < 0,
+                     tile_config=max(config, -1), scale_maps=maps)
+    for rep in range(2):
+        for o in outs:
+            o.fill_(float("nan"))
+        b.run()
+        torch.cuda.synchronize()
+        for o, r in zip(outs, ref):
+            assert torch.equal(o.view(torch.int32), r.view(torch.int32)), rep
+    b.close()
+    if config in (-1, 0):
+        var = ks.variances(s)
+        for x, o, m in zip(xs[::2], outs[::2], maps[::2]):
+            oref, rmap, _ = ob.oracle_forward_f32(x.cpu().numpy(), ko, var, g, want_map=True)
+            assert np.array_equal(o.cpu().numpy().view(np.uint32), oref.view(np.uint32))
+            assert np.array_equal(m.cpu().numpy(), rmap)
