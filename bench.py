@@ -22,9 +22,10 @@ rank's time.
   parity    the GPU image against those reference outputs, bit for bit, on every crop pixel whose
             neighbourhood lies inside its crop
   extra     batched forward (one launch) over 64 images (sides U[256,2048], sigma U[10,40]/255, gamma
-            U[1.5,2.5]) in a CUDA graph, and the adjoint on 8 x 1024^2, each against the plain forward
-            on the same images; forward and adjoint on one 8192^2 image with the gaussian m=(2,0)
-            kernels (sigma 25/255, gamma 1.5); adjoint checked by sum(g*out) = sum(grad*x)
+            U[1.5,2.5]) in a CUDA graph, four 4096^2 images as one plan, and the adjoint on 8 x 1024^2
+            (with the gather's FFMA rate), each against the plain forward on the same images; forward
+            and adjoint on one 8192^2 image with the gaussian m=(2,0) kernels (sigma 25/255, gamma 1.5);
+            adjoint checked by sum(g*out) = sum(grad*x)
 
 --impl reference runs only the reference's CPU engine (bounded sample per step, all host threads).
 """
@@ -481,7 +482,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     if rank == 0:
         peak = fp32_peak()
     if rank == 0 and world == 1 and not args.no_extras:
-        extra = run_extras(torch, lpaici, ks, args, flush)
+        extra = run_extras(torch, lpaici, ks, args, flush, peak)
         # the batched plan on the benchmark image itself, beside the plain launch
         outb = torch.empty_like(x)
         plan = lpaici.Batch(ks, [x], [outb], [SIGMA], [GAMMA], use_graph=True)
@@ -585,7 +586,35 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     shutil.rmtree(tmp, ignore_errors=True)
 
 
-def run_extras(torch, lpaici, ks, args, flush) -> dict:
+def gather_taps_per_px(ks) -> int:
+    """Multiply-adds per output pixel of the adjoint's gather: the taps of the runs of its telescoped
+    kernels D_0 = h_0, D_s = h_s - h_{s-1} (each difference formed in double over the union of the two
+    kernels' boxes and rounded to float, as the library builds them; a run spans a row from its first to
+    its last nonzero)."""
+    w, off, rows, cols = ks.dense()
+    taps = 0
+    for d in range(ks.D):
+        prev = None
+        for s in range(ks.S):
+            k = d * ks.S + s
+            h = w[off[k]:off[k] + rows[k] * cols[k]].reshape(rows[k], cols[k]).astype(np.float64)
+            if prev is not None:
+                hy, hx = max(h.shape[0], prev.shape[0]) // 2, max(h.shape[1], prev.shape[1]) // 2
+                box = np.zeros((2 * hy + 1, 2 * hx + 1))
+                box[hy - h.shape[0] // 2:hy - h.shape[0] // 2 + h.shape[0], hx - h.shape[1] // 2:hx - h.shape[1] // 2 + h.shape[1]] += h
+                box[hy - prev.shape[0] // 2:hy - prev.shape[0] // 2 + prev.shape[0],
+                    hx - prev.shape[1] // 2:hx - prev.shape[1] // 2 + prev.shape[1]] -= prev
+            else:
+                box = h
+            for row in box.astype(np.float32):
+                nz = np.nonzero(row)[0]
+                if len(nz):
+                    taps += int(nz[-1] - nz[0] + 1)
+            prev = h
+    return taps
+
+
+def run_extras(torch, lpaici, ks, args, flush, peak) -> dict:
     import concurrent.futures as cf
 
     from lpaici.synth import mixed_batch
@@ -666,6 +695,7 @@ def run_extras(torch, lpaici, ks, args, flush) -> dict:
         for st, g, o in zip(states, ga, gk):
             lpaici.backward_state(ks, st, g, SIGMA, grad_in=o)
 
+    gtaps = gather_taps_per_px(ks)
     fk_ms = time_launches(torch, fwd_keep, steps, 1, flush)
     ak_ms = time_launches(torch, adj_keep, steps, 1, flush)
     kept_same = all(torch.equal(a.view(torch.int32), b.view(torch.int32)) for a, b in zip(gk, gi))
@@ -689,6 +719,12 @@ def run_extras(torch, lpaici, ks, args, flush) -> dict:
                                            "forward_same_images": m * 1024 * 1024 / (np.mean(f_ms) * 1e-3) / 1e6,
                                            "adjoint_over_forward_time": float(np.mean(a_ms) / np.mean(f_ms))},
                     "identity_rel_err": ident8,
+                    "gather_roofline": {
+                        "taps_per_px": gtaps, "achieved_tflops": 2.0 * gtaps * m * 1024 * 1024 / (np.mean(ak_ms) * 1e-3) / 1e12,
+                        "frac_of_ffma": 2.0 * gtaps * m * 1024 * 1024 / (np.mean(ak_ms) * 1e-3) / peak["ffma_ops_per_s"],
+                        "how": "the gather alone (from kept state, one call per image), 2 FLOP per tap of its "
+                               "telescoped kernels, against the measured FFMA rate; the gather's 1024^2 launches "
+                               "are 1.73 waves of 64x64 tiles"},
                     "kept_state": {"forward_state_over_forward": float(np.mean(fk_ms) / np.mean(f_ms)),
                                    "backward_state_over_forward": float(np.mean(ak_ms) / np.mean(f_ms)),
                                    "bit_equal_to_recomputed": bool(kept_same),
