@@ -66,6 +66,9 @@ struct GatherGeom {
         return g;
     }
     __host__ __device__ size_t cells() const { return static_cast<size_t>(rows) * pitch; }
+    // cells rounded up to whole 4-cell words: the field and the scale map start 16-byte aligned, as the
+    // masking's 16-byte accesses need
+    __host__ __device__ size_t cells4() const { return (cells() + 3) & ~size_t(3); }
 };
 
 // Window of a run over a field: column i is the pair {a[i], b[i]} of the lane's two rows (b = a +
@@ -111,7 +114,7 @@ struct GatherArgs {
 __host__ __device__ inline int rv_words(int nk) { return (nk + 3) & ~3; }
 // The scale map carries 4 bytes past its last cell, set to 0xff: the masking reads it in whole words.
 __host__ __device__ inline size_t gather_smem(int blob_words, int nk, const GatherGeom &g) {
-    return sizeof(int) * (blob_words + rv_words(nk)) + 2 * sizeof(float) * g.cells() + ((g.cells() + 4 + 15) & ~size_t(15));
+    return sizeof(int) * (blob_words + rv_words(nk)) + 2 * sizeof(float) * g.cells4() + ((g.cells4() + 4 + 15) & ~size_t(15));
 }
 
 template <int WY>
@@ -121,12 +124,12 @@ __global__ void __launch_bounds__(GatherShape<WY>::kThreads, 1)
     constexpr int Q = kGatherQ, G = kGatherG;
     extern __shared__ __align__(16) int smem[];
     const int nk = a.D * a.S;
-    const int cells = a.rows * a.pitch;
+    const int cells = a.rows * a.pitch, cells4 = (cells + 3) & ~3;
     int *s_blob = smem;
     float *s_rv = reinterpret_cast<float *>(smem + a.blob_words);
     float *s_u = s_rv + rv_words(nk);  // u = g / den on the halo'd tile, once per tile
-    float *s_f = s_u + cells;          // the field of the current direction
-    uint8_t *s_s = reinterpret_cast<uint8_t *>(s_f + cells);  // s*(d, .) on the halo'd tile
+    float *s_f = s_u + cells4;         // the field of the current direction
+    uint8_t *s_s = reinterpret_cast<uint8_t *>(s_f + cells4);  // s*(d, .) on the halo'd tile
     GatherImage im;
     int tile = blockIdx.x;
     if (a.images) {
@@ -200,19 +203,24 @@ __global__ void __launch_bounds__(GatherShape<WY>::kThreads, 1)
                 const int4 rc = a.rect[k];
                 const unsigned below = 0x01010101u * static_cast<unsigned>(s);
                 __syncthreads();  // every correlation of the previous scale is done with the field
-                // whole 4-cell words of the scale map (a word may reach past the rectangle: zeroing a cell
-                // with s* < s anywhere keeps the field c_d [s* >= s]); 4-byte aligned, as s_s is
-                for (int r = rc.x + warp; r < rc.y; r += nwarps) {
-                    const int w0 = (r * a.pitch + rc.z) >> 2, w1 = (r * a.pitch + rc.w + 3) >> 2;
-                    const unsigned *srow = reinterpret_cast<const unsigned *>(s_s);
-                    for (int wi = w0 + lane; wi < w1; wi += 32) {
-                        const unsigned lt = __vcmpltu4(srow[wi], below);  // 0xff per byte with s* < s
-                        if (lt) {
-                            float *f = s_f + 4 * wi;
-#pragma unroll
-                            for (int b = 0; b < 4; b++)
-                                if (lt & (0xffu << (8 * b))) f[b] = 0.0f;
-                        }
+                // every 4-cell word from the rectangle's first cell to its last, as one flat range over all
+                // threads (the cells beside the rectangle in those rows are masked too: zeroing a cell with
+                // s* < s anywhere keeps the field c_d [s* >= s]).  Per byte, (s* | 0x80) - s keeps its top
+                // bit exactly where s* >= s (scales are below 0x80) and borrows from no other byte; cells
+                // outside this direction's region hold stale bytes, which no correlation reads.
+                const int w0 = (rc.x * a.pitch + rc.z) >> 2, w1 = ((rc.y - 1) * a.pitch + rc.w + 3) >> 2;
+                const unsigned *sw = reinterpret_cast<const unsigned *>(s_s);
+                for (int wi = w0 + static_cast<int>(threadIdx.x); wi < w1; wi += Shape::kThreads) {
+                    const unsigned ge = ((sw[wi] | 0x80808080u) - below) & 0x80808080u;
+                    if (ge != 0x80808080u) {  // a cell of the word has s* < s: keep the others
+                        const unsigned keep = (ge >> 7) * 0xffu;  // 0xff per kept cell
+                        float4 *f4 = reinterpret_cast<float4 *>(s_f) + wi;
+                        float4 v = *f4;
+                        v.x = __uint_as_float(__float_as_uint(v.x) & __byte_perm(keep, 0u, 0x0000));
+                        v.y = __uint_as_float(__float_as_uint(v.y) & __byte_perm(keep, 0u, 0x1111));
+                        v.z = __uint_as_float(__float_as_uint(v.z) & __byte_perm(keep, 0u, 0x2222));
+                        v.w = __uint_as_float(__float_as_uint(v.w) & __byte_perm(keep, 0u, 0x3333));
+                        *f4 = v;
                     }
                 }
                 __syncthreads();
