@@ -6,11 +6,13 @@
 //     c_d(p) = g(p) / den(p) / v_{d, s*(d,p)},
 //     dL/dx(q) = sum_d sum_s sum_t h'_{d,s}(t) [s*(d, q + t) = s] c_d(q + t)       (zero padding)
 // where h' is h mirrored through its centre: for every direction and scale, a correlation of the field
-// masked to the pixels that selected that scale.  Two launches:
+// masked to the pixels that selected that scale.  Three launches:
 //   A. selection: the forward's exact tile sweep recomputes s*(d,p) (one byte per direction and
 //      pixel) and 1/den(p) into a transient workspace -- the forward stores nothing for the adjoint;
-//   B. gather: one CTA per output tile.  It builds u = g / den on the tile plus its R-pixel halo in
-//      shared memory once; per direction it loads s*(d,.) there and forms the field c_d = u / v_{d,s*}.
+//   u: u = g / den over the workspace's 1/den (an elementwise pass; from a kept state the gather forms
+//      the product itself);
+//   B. gather: one CTA per 128 x 64 output tile.  Per direction it reads s*(d,.) and u on the tile plus
+//      its R-pixel halo (from L2) and forms the field c_d = u / v_{d,s*} in shared memory.
 //      The kernels are telescoped, D_s = h'_s - h'_{s-1} (D_0 = h'_0, built by kernelset.cpp), which
 //      turns the sum over scales into
 //          sum_s D_s (*) (c_d [s* >= s]):
@@ -38,23 +40,26 @@ namespace {
 // them as the two halves of packed FMAs; a warp covers 16 rows x 32 columns: lane l has row index
 // a = l & 7 and column group b = l >> 3.  The fields are plain row-major float arrays whose pitch p is
 // 1 mod 8, so the 32 lanes' scalar loads of one row hit 32 different banks (a*p gives the residues
-// mod 8, 8b the multiples of 8).  kGatherWX warps across and WY down make one group; kGatherG groups
-// cover the same outputs, each with every G-th run of a kernel.  Eight columns per lane spread each
-// run's loop, window preload and tail over 16 outputs.
+// mod 8, 8b the multiples of 8).  kGatherWX warps across and WY down make one group; G groups cover
+// the same outputs, each with every G-th run of a kernel: four groups of up to 256 threads, else as
+// many as make 1,024 threads.  Eight columns per lane spread each run's loop, window preload and tail
+// over 16 outputs.
 constexpr int kGatherQ = 8;
 constexpr int kGatherPair = 8;  // rows between a lane's two output rows
-constexpr int kGatherWX = 2;
-constexpr int kGatherG = 4;
+constexpr int kGatherWX = 4;
 constexpr int kGatherWarpCols = 32 / kGatherPair * kGatherQ;  // columns one warp covers
 template <int WY>
 struct GatherShape {
     static constexpr int kTW = kGatherWarpCols * kGatherWX;
     static constexpr int kTH = 2 * kGatherPair * WY;
     static constexpr int kGroupThreads = 32 * kGatherWX * WY;
-    static constexpr int kThreads = kGatherG * kGroupThreads;
+    static constexpr int kG = kGroupThreads > 256 ? 1024 / kGroupThreads : 4;
+    static constexpr int kThreads = kG * kGroupThreads;
 };
-// Tile heights the host can choose (the tallest whose fields and kernels fit in shared memory), four of them.
-constexpr int kGatherWYs[4] = {4, 3, 2, 1};
+// Tile heights the host can choose (the tallest whose field and kernels fit in shared memory): 128 x 64
+// output tiles (two groups of 16 warps) for the 16 x 7 sets with radius 31.
+constexpr int kGatherNWY = 4;
+constexpr int kGatherWYs[kGatherNWY] = {4, 3, 2, 1};
 
 // Field geometry: rows th + 2R, pitch 1 mod 8 and >= tw + 2R + Q (a margin no load reaches).
 struct GatherGeom {
@@ -87,11 +92,12 @@ struct PairWin {
 struct GatherImage {
     const float *g;        // cotangent, pitch g_pitch
     const uint8_t *smap;   // D x H x W selected scales (pass A)
-    const float *rden;     // H x W, pitch W: 1 / den, den = sum_d 1/v_d (pass A)
+    const float *rden;     // H x W, pitch W: 1 / den, den = sum_d 1/v_d (pass A); u = g / den when u_ready
     float *grad;           // result, pitch grad_pitch
     const float *rvar;     // 1 / v_k of this image (batched plans; one image: GatherArgs::rvar)
     int g_pitch, grad_pitch, W, H;
-    int tiles_x, pad;
+    int tiles_x;
+    int u_ready;           // rden holds u = g * (1 / den) already (lpaici_adjoint_u_kernel)
 };
 
 struct GatherArgs {
@@ -110,25 +116,44 @@ struct GatherArgs {
     int4 drect[kMaxKernels];
 };
 
-// Shared memory: blob (runs as field offsets) | 1/v table | u | field | selected scales.
+// Shared memory: blob (runs as field offsets) | 1/v table | field | selected scales.
 __host__ __device__ inline int rv_words(int nk) { return (nk + 3) & ~3; }
 // The scale map carries 4 bytes past its last cell, set to 0xff: the masking reads it in whole words.
 __host__ __device__ inline size_t gather_smem(int blob_words, int nk, const GatherGeom &g) {
-    return sizeof(int) * (blob_words + rv_words(nk)) + 2 * sizeof(float) * g.cells4() + ((g.cells4() + 4 + 15) & ~size_t(15));
+    return sizeof(int) * (blob_words + rv_words(nk)) + sizeof(float) * g.cells4() + ((g.cells4() + 4 + 15) & ~size_t(15));
+}
+
+// Columns [c0, c1) of field row i0 / pitch of a direction's field build, lanes along the row: s*(d, .)
+// into s_s and c_d = u / v_{d,s*} into s_f.  u is read from drow (UReady: u = g / den already) or formed
+// as g * (1/den); cells outside the image get s* = 0 and u = 0.
+template <bool UReady>
+__device__ __forceinline__ void build_field_row(uint8_t *s_s, float *s_f, const float *rv_d, const uint8_t *prow,
+                                                const float *grow, const float *drow, int i0, int c0, int c1, int gx0,
+                                                int W, bool row_ok, int lane) {
+    for (int c = c0 + lane; c < c1; c += 32) {
+        const int gx = gx0 + c;
+        unsigned sc = 0u;
+        float u = 0.0f;
+        if (row_ok && gx >= 0 && gx < W) {
+            sc = __ldg(prow + gx);
+            u = UReady ? __ldg(drow + gx) : __ldg(grow + gx) * __ldg(drow + gx);
+        }
+        s_s[i0 + c] = static_cast<uint8_t>(sc);
+        s_f[i0 + c] = u * rv_d[sc];
+    }
 }
 
 template <int WY>
 __global__ void __launch_bounds__(GatherShape<WY>::kThreads, 1)
     lpaici_adjoint_gather_kernel(const __grid_constant__ GatherArgs a) {
     using Shape = GatherShape<WY>;
-    constexpr int Q = kGatherQ, G = kGatherG;
+    constexpr int Q = kGatherQ, G = Shape::kG;
     extern __shared__ __align__(16) int smem[];
     const int nk = a.D * a.S;
     const int cells = a.rows * a.pitch, cells4 = (cells + 3) & ~3;
     int *s_blob = smem;
     float *s_rv = reinterpret_cast<float *>(smem + a.blob_words);
-    float *s_u = s_rv + rv_words(nk);  // u = g / den on the halo'd tile, once per tile
-    float *s_f = s_u + cells4;         // the field of the current direction
+    float *s_f = s_rv + rv_words(nk);  // the field of the current direction
     uint8_t *s_s = reinterpret_cast<uint8_t *>(s_f + cells4);  // s*(d, .) on the halo'd tile
     GatherImage im;
     int tile = blockIdx.x;
@@ -158,18 +183,6 @@ __global__ void __launch_bounds__(GatherShape<WY>::kThreads, 1)
     stage_blob(s_blob, a.blob, a.blob_words, a.run_word, a.weight_word, a.pitch);
     for (int k = threadIdx.x; k < nk; k += blockDim.x) s_rv[k] = rvar_k[k];
     if (threadIdx.x < 4) s_s[cells + threadIdx.x] = 0xff;  // never below a scale: the masking leaves it
-    for (int r = warp; r < a.rows; r += nwarps) {  // one warp per row, lanes along it
-        const int gy = gy0 + r;
-        const bool row_ok = gy >= 0 && gy < im.H;
-        for (int c = lane; c < a.pitch; c += 32) {
-            const int gx = gx0 + c;
-            float u = 0.0f;
-            if (row_ok && gx >= 0 && gx < im.W)
-                u = __ldg(im.g + static_cast<size_t>(gy) * im.g_pitch + gx) *
-                    __ldg(im.rden + static_cast<size_t>(gy) * im.W + gx);
-            s_u[r * a.pitch + c] = u;
-        }
-    }
 
     float2 acc[Q];
 #pragma unroll
@@ -177,23 +190,24 @@ __global__ void __launch_bounds__(GatherShape<WY>::kThreads, 1)
     const FmaTap tap;
 
     for (int d = 0; d < a.D; d++) {
-        __syncthreads();  // u and the tables staged; the previous direction's correlations are done
-        // s*(d, .) and c_d = u / v_{d, s*} where the direction's kernels reach (u is 0 outside the
-        // image); the other cells keep stale values that no correlation of this direction reads
+        __syncthreads();  // the tables staged; the previous direction's correlations are done
+        // s*(d, .) and c_d = u / v_{d, s*}, u = g / den (0 outside the image), where the direction's
+        // kernels reach; the other cells keep stale values that no correlation of this direction reads.
+        // u is read again for every direction (from L2) instead of being kept in shared memory, which
+        // leaves room for 128-row tiles
         const uint8_t *plane = im.smap + static_cast<size_t>(d) * im.H * im.W;
         const float *rv_d = s_rv + d * a.S;
         const int4 dr = a.drect[d];
         for (int r = dr.x + warp; r < dr.y; r += nwarps) {
             const int gy = gy0 + r;
             const bool row_ok = gy >= 0 && gy < im.H;
-            const uint8_t *prow = plane + static_cast<size_t>(row_ok ? gy : 0) * im.W;
-            for (int c = dr.z + lane; c < dr.w; c += 32) {
-                const int gx = gx0 + c;
-                const unsigned sc = row_ok && gx >= 0 && gx < im.W ? __ldg(prow + gx) : 0u;
-                const int i = r * a.pitch + c;
-                s_s[i] = static_cast<uint8_t>(sc);
-                s_f[i] = s_u[i] * rv_d[sc];
-            }
+            const size_t row = static_cast<size_t>(row_ok ? gy : 0);
+            const uint8_t *prow = plane + row * im.W;
+            const float *grow = im.g + row * im.g_pitch, *drow = im.rden + row * im.W;
+            if (im.u_ready)
+                build_field_row<true>(s_s, s_f, rv_d, prow, grow, drow, r * a.pitch, dr.z, dr.w, gx0, im.W, row_ok, lane);
+            else
+                build_field_row<false>(s_s, s_f, rv_d, prow, grow, drow, r * a.pitch, dr.z, dr.w, gx0, im.W, row_ok, lane);
         }
         __syncthreads();
         // telescoped scales: zero the field where s* < s, as far as D_s reaches, then correlate
@@ -264,14 +278,37 @@ __global__ void __launch_bounds__(GatherShape<WY>::kThreads, 1)
     }
 }
 
+// u = g * (1 / den) written over 1 / den, once per image between the two passes of the recomputing
+// adjoints (the 1/den map is their own workspace there), so that the gather's per-direction field builds
+// read one map instead of two.  The product is the one the gather forms otherwise.  Images blockIdx.y,
+// blockIdx.y + gridDim.y, ... of a batched plan (images: n descriptors), else the single one.
+__global__ void lpaici_adjoint_u_kernel(const GatherImage *images, const GatherImage single, int n) {
+    for (int i = blockIdx.y; i < n; i += gridDim.y) {
+        const GatherImage im = images ? images[i] : single;
+        float *u = const_cast<float *>(im.rden);
+        for (int y = blockIdx.x; y < im.H; y += gridDim.x) {
+            const float *grow = im.g + static_cast<size_t>(y) * im.g_pitch;
+            float *urow = u + static_cast<size_t>(y) * im.W;
+            for (int x = threadIdx.x; x < im.W; x += blockDim.x) urow[x] = grow[x] * urow[x];
+        }
+    }
+}
+
+int u_launch(const GatherImage *images, const GatherImage &single, int n, int max_h, cudaStream_t stream) {
+    const dim3 grid(static_cast<unsigned>(std::min(max_h, 1184)), static_cast<unsigned>(std::min(n, 65535)));
+    lpaici_adjoint_u_kernel<<<grid, 256, 0, stream>>>(images, single, n);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? LPAICI_OK : cuda_error(e, "adjoint u launch");
+}
+
 }  // namespace
 
 namespace {
 
-// The gather kernel of tile height index I .. 3 whose WY is wy (null when none is).
+// The gather kernel of tile height index I .. kGatherNWY - 1 whose WY is wy (null when none is).
 template <int I>
 const void *gather_fn(int wy) {
-    if constexpr (I < 4) {
+    if constexpr (I < kGatherNWY) {
         if (wy == kGatherWYs[I]) return reinterpret_cast<const void *>(lpaici_adjoint_gather_kernel<kGatherWYs[I]>);
         return gather_fn<I + 1>(wy);
     } else {
@@ -281,7 +318,7 @@ const void *gather_fn(int wy) {
 
 template <int I>
 bool gather_launch_at(const GatherArgs &ga, int wy, unsigned grid, size_t smem, cudaStream_t stream) {
-    if constexpr (I < 4) {
+    if constexpr (I < kGatherNWY) {
         constexpr int WY = kGatherWYs[I];
         if (wy != WY) return gather_launch_at<I + 1>(ga, wy, grid, smem, stream);
         lpaici_adjoint_gather_kernel<WY><<<grid, GatherShape<WY>::kThreads, smem, stream>>>(ga);
@@ -382,7 +419,7 @@ long gather_tiles(int width, int height, int th, int *tiles_x) {
 
 int gather_pass(const lpaici_kernelset *ks, const int *adj_blob, const uint8_t *smap, const float *rden,
                 const float *d_grad_out, int gout_pitch, float *d_grad_in, int gin_pitch, int width, int height,
-                float sigma, cudaStream_t stream);
+                float sigma, bool u_ready, cudaStream_t stream);
 
 // The two passes over caller-provided storage (lpaici_backward, lpaici_backward_noalloc).
 int adjoint_passes(const lpaici_kernelset *ks, const int *blob, const int *adj_blob, uint8_t *smap, float *rden,
@@ -407,18 +444,23 @@ int adjoint_passes(const lpaici_kernelset *ks, const int *blob, const int *adj_b
     KernelTables tab;
     fill_tables(ks, nullptr, sigma, gamma, &tab);
     tab.blob = blob;
-    const int rc = launch_forward(ks, img, tab, config_for(ks, width, height), stream);
+    int rc = launch_forward(ks, img, tab, config_for(ks, width, height), stream);
+    if (rc != LPAICI_OK) return rc;
+    // u = g / den over the workspace's 1/den
+    rc = u_launch(nullptr, GatherImage{d_grad_out, smap, rden, d_grad_in, nullptr, gout_pitch, gin_pitch, width, height, 0, 0},
+                  1, height, stream);
     if (rc != LPAICI_OK) return rc;
 
     // B. gather
     return gather_pass(ks, adj_blob, smap, rden, d_grad_out, gout_pitch, d_grad_in, gin_pitch, width, height, sigma,
-                       stream);
+                       true, stream);
 }
 
-// Pass B alone, from the s* planes and 1/den of the image (pass A's outputs or a kept state).
+// Pass B alone, from the s* planes and 1/den of the image (pass A's outputs or a kept state), or u = g / den
+// in place of 1/den (u_ready).
 int gather_pass(const lpaici_kernelset *ks, const int *adj_blob, const uint8_t *smap, const float *rden,
                 const float *d_grad_out, int gout_pitch, float *d_grad_in, int gin_pitch, int width, int height,
-                float sigma, cudaStream_t stream) {
+                float sigma, bool u_ready, cudaStream_t stream) {
     GatherArgs ga{};
     size_t smem = 0;
     int wy = 0;
@@ -429,7 +471,8 @@ int gather_pass(const lpaici_kernelset *ks, const int *adj_blob, const uint8_t *
     if (tiles > 0x7fffffffL) return set_error(LPAICI_ERR_UNSUPPORTED, "image too large: %d x %d", width, height);
     KernelTables tab;
     fill_tables(ks, nullptr, sigma, 1.0f, &tab);
-    ga.single = GatherImage{d_grad_out, smap, rden, d_grad_in, nullptr, gout_pitch, gin_pitch, width, height, tiles_x, 0};
+    ga.single = GatherImage{d_grad_out, smap, rden, d_grad_in, nullptr, gout_pitch, gin_pitch, width, height, tiles_x,
+                            u_ready ? 1 : 0};
     for (int k = 0; k < ks->D * ks->S; k++) ga.rvar[k] = 1.0f / tab.var[k];
     return gather_launch(ga, wy, static_cast<unsigned>(tiles), smem, stream);
 }
@@ -549,6 +592,7 @@ struct lpaici_backward_batch {
     size_t smem = 0;
     int wy = 0;
     unsigned grid = 0;
+    int n = 0, max_h = 0;  // images; the tallest one's rows (the u launch)
     bool use_graph = false;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -558,6 +602,8 @@ namespace {
 
 int backward_batch_enqueue(lpaici_backward_batch *b, cudaStream_t stream) {
     int rc = batch_plan_enqueue(b->select, stream);
+    if (rc != LPAICI_OK) return rc;
+    rc = u_launch(b->ga.images, GatherImage{}, b->n, b->max_h, stream);
     if (rc != LPAICI_OK) return rc;
     return gather_launch(b->ga, b->wy, b->grid, b->smem, stream);
 }
@@ -646,7 +692,8 @@ extern "C" int lpaici_backward_batch_create(const lpaici_kernelset *ks, const lp
         for (int k = 0; k < nk; k++) rv[k] = 1.0f / tab.var[k];
         desc[i] = GatherImage{im.grad_out, smap, rden, im.grad_in,
                               reinterpret_cast<const float *>(base + rvar_off) + static_cast<size_t>(i) * nk,
-                              im.gout_pitch, im.gin_pitch, im.width, im.height, tiles_x[i], 0};
+                              im.gout_pitch, im.gin_pitch, im.width, im.height, tiles_x[i], 1};
+        b->max_h = std::max(b->max_h, im.height);
         int tx = 0;
         const long t = gather_tiles(im.width, im.height, b->ga.th, &tx);
         for (long j = 0; j < t; j++) items.push_back(make_int2(i, static_cast<int>(j)));
@@ -663,6 +710,7 @@ extern "C" int lpaici_backward_batch_create(const lpaici_kernelset *ks, const lp
     b->ga.images = reinterpret_cast<const GatherImage *>(base + desc_off);
     b->ga.items = reinterpret_cast<const int2 *>(base + item_off);
     b->grid = static_cast<unsigned>(total_tiles);
+    b->n = n;
 
     int config = opts ? opts->tile_config : -1;
     if (config < 0) {
@@ -800,5 +848,5 @@ extern "C" int lpaici_backward_state(const lpaici_kernelset *ks, const void *d_s
     const float *rden =
         reinterpret_cast<const float *>(static_cast<const char *>(d_state) + state_smap_bytes(ks, width, height));
     return gather_pass(ks, adj, smap, rden, d_grad_out, gout_pitch, d_grad_in, gin_pitch, width, height, sigma,
-                       reinterpret_cast<cudaStream_t>(stream_));
+                       false, reinterpret_cast<cudaStream_t>(stream_));
 }
