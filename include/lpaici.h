@@ -272,8 +272,8 @@ typedef struct lpaici_backward_batch lpaici_backward_batch;
 
 /* Plans the adjoint of many images: pass A (selection) as one launch over all images'
  * tiles (the forward batch kernel writing s* and 1/den into memory the plan owns, D+4 bytes per
- * pixel), pass B (gather) as one launch over all images' tiles; with use_graph both are captured in
- * one CUDA graph.  Gradients equal lpaici_backward's, image by image, bit for bit.  The pointers are
+ * pixel), u = g/den over the plan's 1/den maps as one elementwise launch, pass B (gather) as one launch
+ * over all images' tiles; with use_graph all three are captured in one CUDA graph.  Gradients equal lpaici_backward's, image by image, bit for bit.  The pointers are
  * baked in: rerun when the contents change, re-plan when the pointers change.  No counterpart in the
  * reference. */
 int lpaici_backward_batch_create(const lpaici_kernelset *ks, const lpaici_grad_image *images, int n,
