@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(GatherShape<WY>::kThreads, 1)
         // s*(d, .) and c_d = u / v_{d, s*}, u = g / den (0 outside the image), where the direction's
         // kernels reach; the other cells keep stale values that no correlation of this direction reads.
         // u is read again for every direction (from L2) instead of being kept in shared memory, which
-        // leaves room for 128-row tiles
+        // leaves room for 128 x 64 tiles
         const uint8_t *plane = im.smap + static_cast<size_t>(d) * im.H * im.W;
         const float *rv_d = s_rv + d * a.S;
         const int4 dr = a.drect[d];
