@@ -12,7 +12,7 @@
 
 namespace lpaici {
 
-// Limits of this build.  The per-kernel variance and threshold tables travel as kernel
+// Limits of this library.  The per-kernel variance and threshold tables travel as kernel
 // parameters (2 * 4 B * kMaxKernels), so D*S is capped; the radius bounds the shared-memory halo.
 constexpr int kMaxKernels = 256;
 constexpr int kMaxRadius = 127;
